@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 FDTD stepping engine.
+
+Default workload (config 3): 384^3 cells at 10 nm with a 12-cell CPML, float32
+fields, a Drude / two-pole Lorentz / eps 2.1 dielectric mix in 8^3 blocks
+(ADE on about two thirds of the cells), an Ex Gaussian dipole, six
+full-plane flux monitors and an Ex/Ey DFT monitor at 8 wavelengths, all
+accumulated on the device every step. One step = one full Yee + CPML + ADE
+time step of the whole domain with its sources and monitors. The stepping
+state (about 6 GB) is far larger than L2, so no L2 flush is needed between
+timed steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0). value = Mcell-updates/s of the whole job,
+timed with CUDA events on the engine's stream (max over ranks). With N > 1
+every rank steps its own replica of the workload (the single-domain path
+does not shard; replicas only), so scaling is weak.
+
+--impl reference times the reference's CPU algorithm for the same workload:
+the NumPy restatement in oracle/ (the reference package itself is Python
+and not present where this runs), on a bounded sample of full-domain steps.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-updates/s (3D Yee+CPML+ADE, fp32)"
+UNIT = "Mcell-updates/s"
+WORKLOAD = ("config3: 384^3 cells (12-cell CPML inside), dx 10 nm, float32, Drude / "
+            "2-pole Lorentz / eps 2.1 media in 8^3 blocks, Ex dipole, 6 full-plane flux "
+            "monitors + Ex/Ey DFT at 8 wavelengths accumulated every step")
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=300)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    p.add_argument("--kernel", default="auto", choices=("auto", "split", "fused"))
+    p.add_argument("--size", type=int, default=384, help="cells per axis (default 384)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def make_sim(pf, size, n_steps):
+    from photonfdtd_b200 import workloads as W
+    return W.config3(pf, n_total=size, block=8, n_steps=n_steps)
+
+
+# --------------------------------------------------------------------------- #
+# Algorithmic bytes per cell-update (compulsory traffic of one unblocked step):
+# 6 fields read + written, one ce per cell, 1 B material id, each CPML psi
+# element read + written, each ADE pole's P^n, P^{n-1} (3 components) read
+# and written: 48 B per pole in float32.
+# --------------------------------------------------------------------------- #
+def algorithmic_bytes(t) -> dict:
+    s = np.dtype(t["npdt"]).itemsize
+    shape = t["shape"]
+    ncell = int(np.prod(shape))
+    n_psi = 0
+    curl = {"Hx": ((1, 2)), "Hy": ((2, 0)), "Hz": ((0, 1)),
+            "Ex": ((1, 2)), "Ey": ((2, 0)), "Ez": ((0, 1))}
+    for comp, axes in curl.items():
+        is_e = comp[0] == "E"
+        ext = []
+        for a in range(3):
+            n = shape[a]
+            ext.append(n - 1 if (a in axes and n > 1) else n)
+        for ax in axes:
+            if shape[ax] <= 1:
+                continue
+            c = t["cpml"][ax][1] if is_e else t["cpml"][ax][3]
+            c = c[1:] if is_e else c[:-1]
+            others = [ext[a] for a in range(3) if a != ax]
+            n_psi += int((c != 0).sum()) * others[0] * others[1]
+    poles = 0.0
+    if t["ade"] is not None:
+        poles = float((t["ade"]["count"] * t["ade"]["npole"]).sum()) / ncell
+    n_ce = 3 if t["ce_mode"] == 1 else 1
+    per_cell = 6 * 2 * s + n_ce * s + n_psi / ncell * 2 * s
+    if t["ade"] is not None:
+        per_cell += 1 + poles * 3 * 2 * 2 * s
+    return dict(per_cell=per_cell, n_psi=n_psi, poles_per_cell=poles, ncell=ncell)
+
+
+# --------------------------------------------------------------------------- #
+class ClockSampler:
+    """nvidia-smi SM clock and throttle reasons while the timed region runs."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.25)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_record(kernel_kind):
+    """DRAM bytes per step of the step kernels from a committed ncu summary,
+    if one exists for this workload (profiles/traffic.json)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(kernel_kind)
+    except (OSError, ValueError):
+        return None
+
+
+# --------------------------------------------------------------------------- #
+def cpu_baseline(size, steps=2):
+    """The oracle (NumPy restatement of the reference CPU path) on full-domain
+    steps of the same workload; one core (NumPy ufuncs are single-threaded)."""
+    import photonfdtd_b200 as pf
+    from oracle import OracleRun
+    sim = make_sim(pf, size, 3000)
+    run = OracleRun(sim)
+    run.advance(1)  # warm-up: first-touch allocations
+    t0 = time.perf_counter()
+    run.advance(steps)
+    wall = time.perf_counter() - t0
+    ncell = int(np.prod(run.shape))
+    return {"value": ncell * steps / wall / 1e6, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{steps} full-domain steps of the {size}^3 workload after 1 warm-up step "
+                      f"({wall:.1f} s), oracle/fdtd_oracle.py (NumPy)"}
+
+
+def run_reference(args):
+    """--impl reference: rank 0 times the CPU algorithm; other ranks idle."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    k = max(1, min(args.steps, 3))
+    base = cpu_baseline(args.size, steps=k)
+    line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": k, "warmup": 1, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": args.size ** 3},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- #
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    import photonfdtd_b200 as pf
+    from photonfdtd_b200 import _native as N
+    from photonfdtd_b200.engine import B200Engine, build_tables
+
+    kern = {"auto": N.PF_KERNEL_AUTO, "split": N.PF_KERNEL_SPLIT,
+            "fused": N.PF_KERNEL_FUSED}[args.kernel]
+    n_total = max(3000, args.warmup + 2 * args.steps + 8)
+    sim = make_sim(pf, args.size, n_total)
+    t = build_tables(sim)
+    alg = algorithmic_bytes(t)
+    eng = B200Engine(t, kernel=kern)
+    stream = torch.cuda.ExternalStream(eng.stream())
+
+    # warm-up, then K timed steps bracketed by barrier + synchronize
+    eng.advance(0, args.warmup)
+    pos = args.warmup
+    eng.read_profile(reset=True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        eng.advance(pos, args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    pos += args.steps
+    ms = ev0.elapsed_time(ev1)
+    launches, _ = eng.read_profile(reset=True)
+    if dist is not None:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        dist.barrier()
+    value = world * alg["ncell"] * args.steps / (ms / 1e3) / 1e6
+
+    # roofline of the step kernels: a second pass with per-launch events
+    eng.set_profiling(True)
+    kp = min(args.steps, 100)
+    eng.advance(pos, kp)
+    pos += kp
+    plaunch, pms = eng.read_profile(reset=True)
+    eng.set_profiling(False)
+    step_ms = pms[0] / kp
+    peak, peak_kind = peaks()
+    achieved = alg["per_cell"] * alg["ncell"] / (step_ms / 1e3) / 1e9
+    kind = "fused" if t["shape"][2] > 1 and plaunch[0] == kp else "split_h+e"
+    tr = traffic_record(f"config3_{args.size}_{kind}")
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": tr,
+            "peak_source": peak_kind,
+            "kernel": ("fused H+E step" if kind == "fused" else "split H and E passes") +
+                      f", {plaunch[0] // kp} launch(es) per step",
+            "step_kernels_ms_per_step": round(step_ms, 4),
+            "algorithmic_bytes_per_cell": round(alg["per_cell"], 2),
+            "monitor_ms_per_step": round((pms[1] + pms[2] + pms[3]) / kp, 4)}
+
+    # end to end through the C ABI with host buffers: upload tables, step,
+    # read the monitor results back
+    e2e = None
+    if not args.no_e2e:
+        eng.close()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2 = B200Engine(t, kernel=kern)
+        e2.advance(0, args.steps)
+        d2h = 0
+        for k, d in enumerate(t["dft"]):
+            for c in d["m"].components:
+                d2h += e2.read_dft(k, c, d["omega"].size, d["counts"]).nbytes
+        for k in range(len(t["flux"])):
+            e2.read_flux(k)
+            d2h += 8
+        wall = time.perf_counter() - t0
+        h2d = e2_upload_bytes(t)
+        e2.close()
+        if dist is not None:
+            tt = torch.tensor([wall], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            wall = float(tt.item())
+        e2e = {"value": round(world * alg["ncell"] * args.steps / wall / 1e6, 2), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d / args.steps),
+               "d2h_bytes_per_step": int(d2h / args.steps),
+               "what": f"engine create + table upload from host memory, {args.steps} steps, "
+                       "DFT + flux read-back, wall clock"}
+    else:
+        eng.close()
+
+    line = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": alg["ncell"], "grid": list(t["shape"]),
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "state ~6 GB > 126 MB L2: inputs larger than L2, no flush"},
+            "roofline": roof, "e2e": e2e, "gpu_launches": int(sum(launches)),
+            "clocks": clk.summary()}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.size)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def e2e_upload_bytes(t) -> int:
+    n = 0
+    if t["ce_mode"] == 2:
+        n += t["word"].nbytes + t["table"].nbytes
+    else:
+        n += sum(a.nbytes for a in t["ce"])
+    for ax in t["cpml"]:
+        n += sum(a.nbytes for a in ax)
+    if t["ade"] is not None and t["ade"]["cell_word"] is not None:
+        n += t["ade"]["cell_word"].nbytes
+    s = t["sources"]
+    n += s["wave"].nbytes + s["amp"].nbytes + s["cell"].nbytes
+    for d in t["dft"]:
+        n += d["ph_e"].nbytes + d["ph_h"].nbytes
+    return n
+
+
+e2_upload_bytes = e2e_upload_bytes
+
+if __name__ == "__main__":
+    main()

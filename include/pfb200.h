@@ -1,0 +1,187 @@
+/*
+ * pfb200.h - C ABI of the B200 FDTD stepping engine (libpfb200.so).
+ *
+ * This is the boundary a photonfdtd backend binds to (ctypes in
+ * photonfdtd_b200/_native.py). It replaces the reference's PyO3 stepper
+ * surface: rust/src/lib.rs:68-133 (step_range_f32/f64) and
+ * rust/src/cuda.rs:512-564 (CudaStepper new_f32/new_f64, run_steps,
+ * read_field), driven by src/photonfdtd/rustbackend.py:237-304 (_CudaEngine).
+ *
+ * Conventions
+ *  - Every field array is C-order (nx, ny, nz), z fastest, in the engine's
+ *    real type (real_bytes 4 = float, 8 = double). Component codes are
+ *    0..5 = Ex, Ey, Ez, Hx, Hy, Hz (rust/src/lib.rs:41-47,
+ *    src/photonfdtd/rustbackend.py:40).
+ *  - Host arrays passed to pf_set_* are borrowed for the duration of the call
+ *    only; the engine copies what it needs. The engine owns all device memory.
+ *  - Every call returns PF_OK (0) or a negative PF_ERR_* code; the message is
+ *    in pf_last_error(). This mirrors the reference mapping CUDA failures to
+ *    RuntimeError("CUDA error: ...") (rust/src/cuda.rs:267-269).
+ *  - One engine = one CUDA stream on the device current at pf_create. Calls on
+ *    one engine must not overlap; different engines are independent.
+ *    pf_advance returns after the stream has synchronised, like run_steps
+ *    (rust/src/cuda.rs:298-341).
+ */
+#ifndef PFB200_H
+#define PFB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PF_OK 0
+#define PF_ERR_INVALID (-1)     /* bad argument or call order           */
+#define PF_ERR_CUDA (-2)        /* a CUDA runtime call failed           */
+#define PF_ERR_OOM (-3)         /* device allocation failed             */
+#define PF_ERR_NONFINITE (-4)   /* non-finite field found by pf_check   */
+#define PF_ERR_UNSUPPORTED (-6) /* feature combination not implemented  */
+#define PF_ERR_STATE (-7)       /* engine not finalised / finalised     */
+
+/* E-update coefficient encodings (pf_set_ce). */
+#define PF_CE_CELL1 0 /* one per-cell array dt/(eps*eps0) for Ex, Ey, Ez  */
+#define PF_CE_CELL3 1 /* three per-cell arrays (diagonal subpixel tensor)  */
+#define PF_CE_TABLE 2 /* per-cell uint32 word indexing a coefficient table */
+
+/* Stepping kernels (pf_set_kernel). */
+#define PF_KERNEL_AUTO 0  /* fused single-pass kernel where it applies     */
+#define PF_KERNEL_SPLIT 1 /* separate H and E passes, one thread per cell  */
+#define PF_KERNEL_FUSED 2 /* require the fused H+E pass (3D only)          */
+
+typedef struct pf_engine pf_engine;
+
+/* Library version string, e.g. "pfb200 0.1.0 sm_100a". */
+const char *pf_version(void);
+
+/* Last error message of an engine (or of the last failed pf_create when
+ * eng is NULL). Never NULL. */
+const char *pf_last_error(const pf_engine *eng);
+
+/* New engine on the current CUDA device.
+ * dx, dy, dz: derivative spacing per axis (1.0 on a collapsed axis, as
+ * src/photonfdtd/simulation.py:912). ch: H-update coefficient dt/mu0 already
+ * rounded to the real type (simulation.py:954). n_steps: length of the run,
+ * bounds the source-waveform and DFT-phase tables.
+ * Replaces CudaStepper::new_f32/new_f64 (rust/src/cuda.rs:512-540). */
+int pf_create(int nx, int ny, int nz, int real_bytes, double dx, double dy,
+              double dz, double ch, int64_t n_steps, pf_engine **out);
+
+/* E-update coefficients (rust/src/cuda.rs:140-247 takes one scalar field;
+ * simulation.py:956-969 adds the three-component subpixel form).
+ *  PF_CE_CELL1: ce0 = nx*ny*nz reals, ce1 = ce2 = NULL.
+ *  PF_CE_CELL3: ce0/ce1/ce2 = per-component arrays for Ex/Ey/Ez.
+ *  PF_CE_TABLE: word = nx*ny*nz uint32; word w < 2^31 selects table[w] (the
+ *    word must be < n_table); w >= 2^31 marks a dispersive cell whose
+ *    coefficient comes from its medium (pf_set_ade). table = n_table reals
+ *    given as doubles (each exactly representable in the real type). */
+int pf_set_ce(pf_engine *eng, int mode, const void *ce0, const void *ce1,
+              const void *ce2, const uint32_t *word, int n_table,
+              const double *table);
+
+/* CPML along one axis (0, 1, 2): b/c on the E and H staggers, n reals each,
+ * in the real type (src/photonfdtd/boundaries.py:31-97 builds them in f64;
+ * simulation.py:1226-1227 casts them). psi is stored only where c != 0,
+ * compacted along the axis as rustbackend._pml_map does (rustbackend.py:126-132).
+ * NULL arrays mean no PML on that axis. */
+int pf_set_cpml(pf_engine *eng, int axis, const void *b_e, const void *c_e,
+                const void *b_h, const void *c_h);
+
+/* Dispersive (ADE) media (simulation.py:572-669). n_media <= 16.
+ *  cell_word: PF_CE_TABLE mode: NULL (the ce word carries the dispersive
+ *    index); PF_CE_CELL1 mode: nx*ny*nz uint32, 0 = non-dispersive, else
+ *    1 + compact index.
+ *  The compact index of a dispersive cell runs over media in order: medium m
+ *  owns [base[m], base[m] + count[m]); within a medium cells are in C order.
+ *  npole[m] <= 8; coef holds, per medium, per pole, (a, b, c) as doubles;
+ *  inv_eps[m] = 1/(eps0*eps_inf); ce_m[m] = the medium's coefficient in table
+ *  mode (ignored otherwise). */
+int pf_set_ade(pf_engine *eng, int n_media, const int64_t *base,
+               const int64_t *count, const int32_t *npole, const double *coef,
+               const double *inv_eps, const double *ce_m,
+               const uint32_t *cell_word);
+
+/* Soft point sources (simulation.py:1367-1390; rustbackend.py:151-166).
+ * n_src entries in the reference's source order: comp (0..5), flat cell
+ * index i*ny*nz + j*nz + k, waveform row, amplitude. wave = n_wave rows of
+ * n_steps doubles: row w, column s is the waveform at that source family's
+ * Yee time of step s ((s+1/2)dt for H, (s+1)dt for E). The value added at
+ * step s is amp * wave[w][s], computed in double and added in double before
+ * rounding to the field type, as the reference does. */
+int pf_set_sources(pf_engine *eng, int n_src, const int32_t *comp,
+                   const int64_t *cell, const int32_t *wave_row,
+                   const double *amp, int n_wave, const double *wave);
+
+/* Running DFT monitor (simulation.py:1116-1133; rustbackend.py:384-397).
+ * Region: start/stop/stride per axis (a plane is start = i, stop = i+1).
+ * comp_mask: bit c set = record component c. Sampled at steps
+ * s = 0, interval, 2*interval, ... < n_steps. phase_e / phase_h: one row per
+ * sample, n_freq complex values as (re, im) doubles, = exp(i*omega*t) at the E
+ * and H time of that sample (computed by the host exactly as the reference
+ * does). dt: the Riemann-sum weight. Output id in *mon. */
+int pf_add_dft(pf_engine *eng, const int32_t start[3], const int32_t stop[3],
+               const int32_t stride[3], int comp_mask, int n_freq,
+               int interval, const double *phase_e, const double *phase_h,
+               double dt, int *mon);
+
+/* Poynting flux through the full plane normal to axis at index idx
+ * (simulation.py:1440-1459, accumulated every step as :1403-1406):
+ * flux += real(sum(S) * dA) * dt, S = E_t1*H_t2 - E_t2*H_t1 at the same cell.
+ * The plane sum is taken in double; the product with dA is rounded to the
+ * real type as the reference's float32 run does. */
+int pf_add_flux(pf_engine *eng, int axis, int idx, double dA, double dt,
+                int *mon);
+
+/* Kernel choice (PF_KERNEL_*); default PF_KERNEL_AUTO. */
+int pf_set_kernel(pf_engine *eng, int kernel);
+
+/* Allocate the device state, upload the tables, zero the fields. */
+int pf_finalize(pf_engine *eng);
+
+/* Advance global steps [step0, step0 + n_sub) (rust/src/cuda.rs:298-341,
+ * rustbackend.py:222-231 / 297-299). step0 must equal the engine's step
+ * counter (steps are not skipped or repeated). */
+int pf_advance(pf_engine *eng, int64_t step0, int64_t n_sub);
+
+/* Current value of one field component into host memory, nx*ny*nz reals
+ * (rust/src/cuda.rs:552-564, read_field). */
+int pf_read_field(pf_engine *eng, int comp, void *host_dst);
+
+/* DFT accumulator of monitor mon, component comp: n_freq x region cells
+ * complex128 as interleaved (re, im) doubles (simulation.py:1124-1133). */
+int pf_read_dft(pf_engine *eng, int mon, int comp, double *host_dst);
+
+/* Time-integrated flux of flux monitor mon (simulation.py:1403-1406). */
+int pf_read_flux(pf_engine *eng, int mon, double *host_dst);
+
+/* Steps advanced so far. */
+int pf_step(const pf_engine *eng, int64_t *step);
+
+/* Scan all six fields for non-finite values: PF_OK or PF_ERR_NONFINITE. */
+int pf_check_finite(pf_engine *eng);
+
+/* The CUDA stream (a cudaStream_t) the engine launches on, so a caller can
+ * time its work with events on that stream. */
+int pf_stream(const pf_engine *eng, void **stream);
+
+/* Launch accounting. Kinds: 0 = step passes (H/E or fused), 1 = source
+ * injection, 2 = monitor sampling, 3 = monitor flush. launches[k] counts
+ * every launch; with profiling on (pf_set_profiling), ms[k] sums the device
+ * time of those launches from events recorded around each one. reset != 0
+ * zeroes both after reading. Profiling adds event records between launches,
+ * so time work with it off. */
+int pf_set_profiling(pf_engine *eng, int on);
+int pf_read_profile(pf_engine *eng, int64_t launches[4], double ms[4], int reset);
+
+/* Device bytes held by the engine. */
+int pf_device_bytes(const pf_engine *eng, int64_t *bytes);
+
+/* Release everything. NULL is a no-op. */
+void pf_destroy(pf_engine *eng);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PFB200_H */

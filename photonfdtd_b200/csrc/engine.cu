@@ -1,0 +1,858 @@
+// engine.cu - the C ABI of libpfb200.so (declared in include/pfb200.h).
+//
+// Device state of one engine (all in HBM for the whole run):
+//   fields   2 time levels x 6 components, C-order (nx, ny, nz); a step reads
+//            level `cur` and writes level `cur ^ 1` (the fused kernel
+//            recomputes H on tile halos, so reads and writes must not alias)
+//   ce       one or three per-cell arrays, or a uint32 word per cell + table
+//   CPML     b/c per axis and stagger, compact maps (-1 = no psi), psi
+//            compacted along its derivative axis; H psi double-buffered
+//   ADE      compact polarisation state [level][pole][comp][cells] per medium
+//   monitors sample rings + complex128 accumulators (DFT), block partials +
+//            float64 accumulators (flux)
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pfb200.h"
+#include "common.cuh"
+#include "kernels_aux.cuh"
+#include "kernels_fused.cuh"
+#include "kernels_split.cuh"
+
+using namespace pfb;
+
+namespace {
+
+constexpr int kRingMax = 32;
+constexpr size_t kRingBytesCap = 256u << 20;
+thread_local std::string g_create_error;
+
+struct DftMon {
+  DftRegion r;
+  int n_freq = 0, interval = 1;
+  double dt = 0;
+  std::vector<double> h_ph_e, h_ph_h;
+  long long n_samples = 0;   // samples in the whole run
+  long long q_done = 0;      // samples folded into acc
+  int pending = 0;           // samples waiting in the ring
+  int ring_cap = 1;
+  void* ring = nullptr;
+  double* acc = nullptr;
+  double* ph_e = nullptr;
+  double* ph_h = nullptr;
+};
+
+struct FluxMon {
+  FluxPlane p;
+  double dA = 0, dt = 0;
+  int pending = 0;
+  int ring_cap = kRingMax;
+  double* partial = nullptr;
+  double* acc = nullptr;
+};
+
+struct SrcFamily {
+  std::vector<long long> cell;
+  std::vector<int> comp, start, wave_row;
+  std::vector<double> amp;
+  SourceGroups dev{};
+};
+
+}  // namespace
+
+struct pf_engine {
+  int nx = 0, ny = 0, nz = 0, rb = 4;
+  double dl[3] = {1, 1, 1};
+  double ch = 0;
+  long long n_steps = 0;
+  long long ncell = 0;
+  int kernel = PF_KERNEL_AUTO;
+  bool finalized = false;
+  long long step = 0;
+  int cur = 0;
+  std::string err;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  size_t dev_bytes = 0;
+  std::vector<void*> allocs;
+
+  // staged tables
+  int ce_mode = -1;
+  std::vector<char> h_ce[3];
+  std::vector<uint32_t> h_word;
+  std::vector<double> h_table;
+  std::vector<char> h_cpml[3][4];  // b_e, c_e, b_h, c_h
+  int n_media = 0;
+  std::vector<long long> m_base, m_count;
+  std::vector<int> m_npole;
+  std::vector<double> m_coef, m_inv, m_ce;
+  std::vector<uint32_t> h_adeword;
+  SrcFamily src[2];  // 0 = E family, 1 = H family
+  int n_wave = 0;
+  std::vector<double> h_wave;
+  std::vector<DftMon> dfts;
+  std::vector<FluxMon> fluxes;
+
+  // device
+  void* E[2][3] = {};
+  void* H[2][3] = {};
+  void* ce[3] = {};
+  uint32_t* word = nullptr;
+  void* table = nullptr;
+  uint32_t* adeword = nullptr;
+  void* cp[3][4] = {};
+  int* map_e[3] = {};
+  int* map_h[3] = {};
+  int npe[3] = {}, nph[3] = {};
+  void* psiE[6] = {};
+  void* psiH[2][6] = {};
+  void* P = nullptr;
+  void* media = nullptr;
+  double* wave = nullptr;
+  int* flag = nullptr;
+  bool fused = false;
+
+  // launch accounting (pf_read_profile)
+  long long launches[4] = {};
+  double prof_ms[4] = {};
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, int>> ev_pending;  // (kind, first event)
+  size_t ev_used = 0;
+};
+
+namespace {
+
+int fail(pf_engine* e, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (e)
+    e->err = buf;
+  else
+    g_create_error = buf;
+  return code;
+}
+
+#define PF_CUDA(e, call)                                                                   \
+  do {                                                                                     \
+    cudaError_t rc_ = (call);                                                              \
+    if (rc_ != cudaSuccess)                                                                \
+      return fail((e), rc_ == cudaErrorMemoryAllocation ? PF_ERR_OOM : PF_ERR_CUDA,        \
+                  "CUDA error: %s (%s) at %s:%d", cudaGetErrorString(rc_), #call, __FILE__, \
+                  __LINE__);                                                               \
+  } while (0)
+
+int dalloc(pf_engine* e, void** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t rc = cudaMalloc(p, bytes);
+  if (rc != cudaSuccess)
+    return fail(e, PF_ERR_OOM, "CUDA error: cudaMalloc of %zu bytes failed: %s", bytes,
+                cudaGetErrorString(rc));
+  e->allocs.push_back(*p);
+  e->dev_bytes += bytes;
+  rc = cudaMemsetAsync(*p, 0, bytes, e->stream);
+  if (rc != cudaSuccess) return fail(e, PF_ERR_CUDA, "CUDA error: %s", cudaGetErrorString(rc));
+  return PF_OK;
+}
+
+int upload(pf_engine* e, void** p, const void* src, size_t bytes) {
+  int rc = dalloc(e, p, bytes);
+  if (rc) return rc;
+  if (bytes) PF_CUDA(e, cudaMemcpyAsync(*p, src, bytes, cudaMemcpyHostToDevice, e->stream));
+  return PF_OK;
+}
+
+// Bracket one launch of `kind` (0 step, 1 sources, 2 sampling, 3 flush).
+struct LaunchScope {
+  pf_engine* e;
+  int kind;
+  LaunchScope(pf_engine* eng, int k) : e(eng), kind(k) {
+    e->launches[kind]++;
+    if (!e->profiling) return;
+    while (e->ev_pool.size() < e->ev_used + 2) {
+      cudaEvent_t ev;
+      cudaEventCreate(&ev);
+      e->ev_pool.push_back(ev);
+    }
+    cudaEventRecord(e->ev_pool[e->ev_used], e->stream);
+  }
+  ~LaunchScope() {
+    if (!e->profiling) return;
+    cudaEventRecord(e->ev_pool[e->ev_used + 1], e->stream);
+    e->ev_pending.push_back({kind, (int)e->ev_used});
+    e->ev_used += 2;
+  }
+};
+
+// Fold recorded event pairs into prof_ms (the stream must be idle).
+void collect_profile(pf_engine* e) {
+  for (auto& pr : e->ev_pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, e->ev_pool[pr.second], e->ev_pool[pr.second + 1]) == cudaSuccess)
+      e->prof_ms[pr.first] += ms;
+  }
+  e->ev_pending.clear();
+  e->ev_used = 0;
+}
+
+template <typename T>
+int finalize_typed(pf_engine* e) {
+  const size_t S = sizeof(T);
+  const long long n = e->ncell;
+  const int dims[3] = {e->nx, e->ny, e->nz};
+  int rc;
+  for (int lvl = 0; lvl < 2; ++lvl)
+    for (int c = 0; c < 3; ++c) {
+      if ((rc = dalloc(e, &e->E[lvl][c], n * S))) return rc;
+      if ((rc = dalloc(e, &e->H[lvl][c], n * S))) return rc;
+    }
+  // E coefficients
+  if (e->ce_mode == PF_CE_CELL1) {
+    if ((rc = upload(e, &e->ce[0], e->h_ce[0].data(), n * S))) return rc;
+    e->ce[1] = e->ce[2] = e->ce[0];
+  } else if (e->ce_mode == PF_CE_CELL3) {
+    for (int c = 0; c < 3; ++c)
+      if ((rc = upload(e, &e->ce[c], e->h_ce[c].data(), n * S))) return rc;
+  } else {
+    if ((rc = upload(e, (void**)&e->word, e->h_word.data(), n * 4))) return rc;
+    std::vector<T> tab(e->h_table.size());
+    for (size_t q = 0; q < tab.size(); ++q) tab[q] = (T)e->h_table[q];
+    if ((rc = upload(e, &e->table, tab.data(), tab.size() * S))) return rc;
+  }
+  // CPML: coefficients, compact maps, psi
+  for (int ax = 0; ax < 3; ++ax) {
+    const int na = dims[ax];
+    std::vector<T> arr[4];
+    for (int q = 0; q < 4; ++q) {
+      arr[q].assign(na, T(0));
+      if (!e->h_cpml[ax][q].empty()) memcpy(arr[q].data(), e->h_cpml[ax][q].data(), na * S);
+      if ((rc = upload(e, &e->cp[ax][q], arr[q].data(), na * S))) return rc;
+    }
+    std::vector<int> me(na, -1), mh(na, -1);
+    int ce_n = 0, ch_n = 0;
+    for (int t = 0; t < na; ++t) {
+      if (arr[1][t] != T(0)) me[t] = ce_n++;
+      if (arr[3][t] != T(0)) mh[t] = ch_n++;
+    }
+    e->npe[ax] = ce_n;
+    e->nph[ax] = ch_n;
+    if ((rc = upload(e, (void**)&e->map_e[ax], me.data(), na * 4))) return rc;
+    if ((rc = upload(e, (void**)&e->map_h[ax], mh.data(), na * 4))) return rc;
+  }
+  const long long nx = e->nx, ny = e->ny, nz = e->nz;
+  // psi extents: the term's derivative axis replaced by its PML cell count
+  const long long eE[6] = {nx * e->npe[1] * nz, nx * ny * e->npe[2], nx * ny * e->npe[2],
+                           (long long)e->npe[0] * ny * nz, (long long)e->npe[0] * ny * nz,
+                           nx * e->npe[1] * nz};
+  const long long eH[6] = {nx * e->nph[1] * nz, nx * ny * e->nph[2], nx * ny * e->nph[2],
+                           (long long)e->nph[0] * ny * nz, (long long)e->nph[0] * ny * nz,
+                           nx * e->nph[1] * nz};
+  for (int q = 0; q < 6; ++q) {
+    if ((rc = dalloc(e, &e->psiE[q], eE[q] * S))) return rc;
+    for (int lvl = 0; lvl < 2; ++lvl)
+      if ((rc = dalloc(e, &e->psiH[lvl][q], eH[q] * S))) return rc;
+  }
+  // ADE
+  if (e->n_media > 0) {
+    std::vector<MediumT<T>> md(e->n_media);
+    long long off = 0;
+    size_t ci = 0;
+    for (int m = 0; m < e->n_media; ++m) {
+      MediumT<T>& M = md[m];
+      memset(&M, 0, sizeof M);
+      M.base = e->m_base[m];
+      M.count = e->m_count[m];
+      M.poff = off;
+      M.npole = e->m_npole[m];
+      M.inv = (T)e->m_inv[m];
+      M.ce = (T)e->m_ce[m];
+      for (int p = 0; p < M.npole; ++p) {
+        M.a[p] = (T)e->m_coef[ci++];
+        M.b[p] = (T)e->m_coef[ci++];
+        M.c[p] = (T)e->m_coef[ci++];
+      }
+      off += 2LL * M.npole * 3 * M.count;
+    }
+    if ((rc = dalloc(e, &e->P, off * S))) return rc;
+    if ((rc = upload(e, &e->media, md.data(), md.size() * sizeof(MediumT<T>)))) return rc;
+    if (e->ce_mode == PF_CE_CELL1)
+      if ((rc = upload(e, (void**)&e->adeword, e->h_adeword.data(), n * 4))) return rc;
+    if (e->ce_mode == PF_CE_TABLE && e->m_ce.size() != (size_t)e->n_media)
+      return fail(e, PF_ERR_INVALID, "table mode needs each medium's coefficient");
+  }
+  // sources
+  if (e->n_wave > 0)
+    if ((rc = upload(e, (void**)&e->wave, e->h_wave.data(), e->h_wave.size() * 8))) return rc;
+  for (int f = 0; f < 2; ++f) {
+    SrcFamily& s = e->src[f];
+    SourceGroups& d = s.dev;
+    d.n_groups = (int)s.cell.size();
+    d.n_steps = e->n_steps;
+    d.wave = e->wave;
+    if (d.n_groups == 0) continue;
+    if ((rc = upload(e, (void**)&d.cell, s.cell.data(), s.cell.size() * 8))) return rc;
+    if ((rc = upload(e, (void**)&d.comp, s.comp.data(), s.comp.size() * 4))) return rc;
+    if ((rc = upload(e, (void**)&d.start, s.start.data(), s.start.size() * 4))) return rc;
+    if ((rc = upload(e, (void**)&d.wave_row, s.wave_row.data(), s.wave_row.size() * 4))) return rc;
+    if ((rc = upload(e, (void**)&d.amp, s.amp.data(), s.amp.size() * 8))) return rc;
+  }
+  // monitors
+  for (DftMon& m : e->dfts) {
+    const size_t per = (size_t)m.r.ncomp * m.r.ncell * S;
+    m.ring_cap = (int)std::max<size_t>(1, std::min<size_t>(kRingMax, kRingBytesCap / std::max<size_t>(per, 1)));
+    if ((rc = dalloc(e, &m.ring, per * m.ring_cap))) return rc;
+    if ((rc = dalloc(e, (void**)&m.acc, (size_t)m.r.ncomp * m.n_freq * m.r.ncell * 16))) return rc;
+    if ((rc = upload(e, (void**)&m.ph_e, m.h_ph_e.data(), m.h_ph_e.size() * 8))) return rc;
+    if ((rc = upload(e, (void**)&m.ph_h, m.h_ph_h.data(), m.h_ph_h.size() * 8))) return rc;
+  }
+  for (FluxMon& f : e->fluxes) {
+    if ((rc = dalloc(e, (void**)&f.partial, (size_t)f.ring_cap * f.p.nblk * 8))) return rc;
+    if ((rc = dalloc(e, (void**)&f.acc, 8))) return rc;
+  }
+  if ((rc = dalloc(e, (void**)&e->flag, sizeof(int)))) return rc;
+  PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  return PF_OK;
+}
+
+template <typename T>
+StepArgs<T> step_args(pf_engine* e) {
+  StepArgs<T> a;
+  memset(&a, 0, sizeof a);
+  a.nx = e->nx;
+  a.ny = e->ny;
+  a.nz = e->nz;
+  a.dx = (T)e->dl[0];
+  a.dy = (T)e->dl[1];
+  a.dz = (T)e->dl[2];
+  a.ch = (T)e->ch;
+  const int c0 = e->cur, c1 = e->cur ^ 1;
+  for (int c = 0; c < 3; ++c) {
+    a.Ein[c] = (const T*)e->E[c0][c];
+    a.Hin[c] = (const T*)e->H[c0][c];
+    a.Eout[c] = (T*)e->E[c1][c];
+    a.Hout[c] = (T*)e->H[c1][c];
+    a.ce[c] = (const T*)e->ce[c];
+  }
+  a.word = e->word;
+  a.table = (const T*)e->table;
+  a.adeword = e->adeword;
+  for (int ax = 0; ax < 3; ++ax) {
+    a.be[ax] = (const T*)e->cp[ax][0];
+    a.cpe[ax] = (const T*)e->cp[ax][1];
+    a.bh[ax] = (const T*)e->cp[ax][2];
+    a.cph[ax] = (const T*)e->cp[ax][3];
+    a.mape[ax] = e->map_e[ax];
+    a.maph[ax] = e->map_h[ax];
+    a.npe[ax] = e->npe[ax];
+    a.nph[ax] = e->nph[ax];
+  }
+  for (int q = 0; q < 6; ++q) {
+    a.psiE[q] = (T*)e->psiE[q];
+    a.psiHin[q] = (const T*)e->psiH[c0][q];
+    a.psiHout[q] = (T*)e->psiH[c1][q];
+  }
+  a.media = (const MediumT<T>*)e->media;
+  a.n_media = e->n_media;
+  a.P = (T*)e->P;
+  a.lvl = (int)(e->step & 1);
+  return a;
+}
+
+template <typename T>
+void launch_e_split(pf_engine* e, const StepArgs<T>& a, dim3 g, dim3 b) {
+  const bool ade = e->n_media > 0;
+  switch (e->ce_mode) {
+    case PF_CE_CELL1:
+      if (ade) k_e_split<T, kCeCell1, true><<<g, b, 0, e->stream>>>(a);
+      else k_e_split<T, kCeCell1, false><<<g, b, 0, e->stream>>>(a);
+      break;
+    case PF_CE_CELL3:
+      k_e_split<T, kCeCell3, false><<<g, b, 0, e->stream>>>(a);
+      break;
+    default:
+      if (ade) k_e_split<T, kCeTable, true><<<g, b, 0, e->stream>>>(a);
+      else k_e_split<T, kCeTable, false><<<g, b, 0, e->stream>>>(a);
+  }
+}
+
+template <typename T>
+Fields6<T> level_fields(pf_engine* e, int lvl) {
+  Fields6<T> f;
+  for (int c = 0; c < 3; ++c) {
+    f.f[c] = (const T*)e->E[lvl][c];
+    f.f[3 + c] = (const T*)e->H[lvl][c];
+  }
+  return f;
+}
+
+template <typename T>
+int flush_monitors(pf_engine* e) {
+  for (DftMon& m : e->dfts) {
+    if (m.pending == 0) continue;
+    const long long nt = m.r.ncell * m.r.ncomp;
+    const int B = 128;
+    LaunchScope ls(e, 3);
+    k_dft_flush<T><<<(unsigned)((nt + B - 1) / B), B, 0, e->stream>>>(
+        m.r, (const T*)m.ring, m.pending, m.acc, m.ph_e, m.ph_h, m.q_done, m.n_freq, m.dt);
+    m.q_done += m.pending;
+    m.pending = 0;
+  }
+  for (FluxMon& f : e->fluxes) {
+    if (f.pending == 0) continue;
+    LaunchScope ls(e, 3);
+    k_flux_flush<T><<<1, 256, 0, e->stream>>>(f.partial, f.p.nblk, f.pending, f.acc, f.dA, f.dt);
+    f.pending = 0;
+  }
+  PF_CUDA(e, cudaGetLastError());
+  return PF_OK;
+}
+
+// Monitors of step s read the level just written (E at t_e, H at t_h).
+template <typename T>
+int sample_monitors(pf_engine* e, long long s, int lvl) {
+  if (e->dfts.empty() && e->fluxes.empty()) return PF_OK;
+  const Fields6<T> f = level_fields<T>(e, lvl);
+  for (DftMon& m : e->dfts) {
+    if (s % m.interval) continue;
+    if (m.pending == m.ring_cap) {
+      int rc = flush_monitors<T>(e);
+      if (rc) return rc;
+    }
+    const int B = 256;
+    LaunchScope ls(e, 2);
+    k_dft_sample<T><<<(unsigned)((m.r.ncell + B - 1) / B), B, 0, e->stream>>>(
+        m.r, (T*)m.ring, m.pending, f, e->ny, e->nz);
+    m.pending++;
+  }
+  for (FluxMon& fl : e->fluxes) {
+    if (fl.pending == fl.ring_cap) {
+      int rc = flush_monitors<T>(e);
+      if (rc) return rc;
+    }
+    LaunchScope ls(e, 2);
+    k_flux_sample<T><<<fl.p.nblk, 256, 0, e->stream>>>(fl.p, fl.partial, fl.pending, f, e->ny, e->nz);
+    fl.pending++;
+  }
+  return PF_OK;
+}
+
+template <typename T>
+int inject(pf_engine* e, int fam, int lvl, long long s) {
+  SourceGroups& d = e->src[fam].dev;
+  if (d.n_groups == 0) return PF_OK;
+  void** F = fam == 0 ? e->E[lvl] : e->H[lvl];
+  LaunchScope ls(e, 1);
+  k_inject<T><<<(d.n_groups + 127) / 128, 128, 0, e->stream>>>(d, (T*)F[0], (T*)F[1], (T*)F[2], s);
+  return PF_OK;
+}
+
+template <typename T>
+int advance_typed(pf_engine* e, long long n_sub) {
+  const int nz = e->nz, ny = e->ny, nx = e->nx;
+  const dim3 blk = nz > 1 ? dim3(32, 8) : dim3(1, 256);
+  const dim3 grd((nz + blk.x - 1) / blk.x, (ny + blk.y - 1) / blk.y, nx);
+  for (long long t = 0; t < n_sub; ++t) {
+    const long long s = e->step;
+    const int nxt = e->cur ^ 1;
+    StepArgs<T> a = step_args<T>(e);
+    if (e->fused) {
+      int rc;
+      {
+        LaunchScope ls(e, 0);
+        rc = launch_fused<T>(e->stream, a, e->ce_mode, e->n_media > 0);
+      }
+      if (rc) return fail(e, PF_ERR_UNSUPPORTED, "fused kernel does not cover this case");
+      // sources of the fused path are injected after its single pass: an H
+      // source must reach the E update, so the fused path is only chosen
+      // when there are no H-family sources.
+      inject<T>(e, 0, nxt, s);
+    } else {
+      {
+        LaunchScope ls(e, 0);
+        k_h_split<T><<<grd, blk, 0, e->stream>>>(a);
+      }
+      inject<T>(e, 1, nxt, s);
+      a.Hin[0] = a.Hout[0];
+      a.Hin[1] = a.Hout[1];
+      a.Hin[2] = a.Hout[2];
+      {
+        LaunchScope ls(e, 0);
+        launch_e_split<T>(e, a, grd, blk);
+      }
+      inject<T>(e, 0, nxt, s);
+    }
+    int rc = sample_monitors<T>(e, s, nxt);
+    if (rc) return rc;
+    e->cur = nxt;
+    e->step++;
+  }
+  PF_CUDA(e, cudaGetLastError());
+  PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  collect_profile(e);
+  return PF_OK;
+}
+
+bool valid_comp(int c) { return c >= 0 && c < 6; }
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* pf_version(void) { return "pfb200 0.1.0 sm_100a"; }
+
+const char* pf_last_error(const pf_engine* e) {
+  return e ? e->err.c_str() : g_create_error.c_str();
+}
+
+int pf_create(int nx, int ny, int nz, int real_bytes, double dx, double dy, double dz, double ch,
+              int64_t n_steps, pf_engine** out) {
+  if (!out) return fail(nullptr, PF_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  if (nx < 1 || ny < 1 || nz < 1)
+    return fail(nullptr, PF_ERR_INVALID, "grid shape must be positive, got %d x %d x %d", nx, ny, nz);
+  if (real_bytes != 4 && real_bytes != 8)
+    return fail(nullptr, PF_ERR_INVALID, "real_bytes must be 4 or 8, got %d", real_bytes);
+  if (n_steps < 0) return fail(nullptr, PF_ERR_INVALID, "n_steps must be >= 0");
+  if ((long long)nx * ny * nz > 0x7fffffffLL)
+    return fail(nullptr, PF_ERR_UNSUPPORTED, "more than 2^31-1 cells");
+  if (!(dx > 0 && dy > 0 && dz > 0)) return fail(nullptr, PF_ERR_INVALID, "spacings must be > 0");
+  pf_engine* e = new pf_engine();
+  e->nx = nx;
+  e->ny = ny;
+  e->nz = nz;
+  e->rb = real_bytes;
+  e->dl[0] = dx;
+  e->dl[1] = dy;
+  e->dl[2] = dz;
+  e->ch = ch;
+  e->n_steps = n_steps;
+  e->ncell = (long long)nx * ny * nz;
+  cudaError_t rc = cudaGetDevice(&e->device);
+  if (rc == cudaSuccess) rc = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+  if (rc != cudaSuccess) {
+    fail(nullptr, PF_ERR_CUDA, "CUDA error: %s", cudaGetErrorString(rc));
+    delete e;
+    return PF_ERR_CUDA;
+  }
+  *out = e;
+  return PF_OK;
+}
+
+int pf_set_ce(pf_engine* e, int mode, const void* ce0, const void* ce1, const void* ce2,
+              const uint32_t* word, int n_table, const double* table) {
+  if (!e) return PF_ERR_INVALID;
+  if (e->finalized) return fail(e, PF_ERR_STATE, "pf_set_ce after pf_finalize");
+  const size_t bytes = (size_t)e->ncell * e->rb;
+  for (int c = 0; c < 3; ++c) e->h_ce[c].clear();
+  e->h_word.clear();
+  e->h_table.clear();
+  if (mode == PF_CE_CELL1) {
+    if (!ce0) return fail(e, PF_ERR_INVALID, "PF_CE_CELL1 needs ce0");
+    e->h_ce[0].assign((const char*)ce0, (const char*)ce0 + bytes);
+  } else if (mode == PF_CE_CELL3) {
+    if (!ce0 || !ce1 || !ce2) return fail(e, PF_ERR_INVALID, "PF_CE_CELL3 needs three arrays");
+    const void* src[3] = {ce0, ce1, ce2};
+    for (int c = 0; c < 3; ++c) e->h_ce[c].assign((const char*)src[c], (const char*)src[c] + bytes);
+  } else if (mode == PF_CE_TABLE) {
+    if (!word || n_table < 1 || !table) return fail(e, PF_ERR_INVALID, "PF_CE_TABLE needs word and table");
+    for (long long q = 0; q < e->ncell; ++q)
+      if (!(word[q] & kDispersiveBit) && word[q] >= (uint32_t)n_table)
+        return fail(e, PF_ERR_INVALID, "ce word %u at cell %lld exceeds table size %d", word[q], q, n_table);
+    e->h_word.assign(word, word + e->ncell);
+    e->h_table.assign(table, table + n_table);
+  } else {
+    return fail(e, PF_ERR_INVALID, "unknown ce mode %d", mode);
+  }
+  e->ce_mode = mode;
+  return PF_OK;
+}
+
+int pf_set_cpml(pf_engine* e, int axis, const void* b_e, const void* c_e, const void* b_h,
+                const void* c_h) {
+  if (!e) return PF_ERR_INVALID;
+  if (e->finalized) return fail(e, PF_ERR_STATE, "pf_set_cpml after pf_finalize");
+  if (axis < 0 || axis > 2) return fail(e, PF_ERR_INVALID, "axis must be 0..2");
+  const int dims[3] = {e->nx, e->ny, e->nz};
+  const size_t bytes = (size_t)dims[axis] * e->rb;
+  const void* src[4] = {b_e, c_e, b_h, c_h};
+  for (int q = 0; q < 4; ++q) {
+    e->h_cpml[axis][q].clear();
+    if (src[q]) e->h_cpml[axis][q].assign((const char*)src[q], (const char*)src[q] + bytes);
+  }
+  return PF_OK;
+}
+
+int pf_set_ade(pf_engine* e, int n_media, const int64_t* base, const int64_t* count,
+               const int32_t* npole, const double* coef, const double* inv_eps, const double* ce_m,
+               const uint32_t* cell_word) {
+  if (!e) return PF_ERR_INVALID;
+  if (e->finalized) return fail(e, PF_ERR_STATE, "pf_set_ade after pf_finalize");
+  if (n_media < 0 || n_media > kMaxMedia)
+    return fail(e, PF_ERR_UNSUPPORTED, "at most %d dispersive media, got %d", kMaxMedia, n_media);
+  e->n_media = n_media;
+  e->m_base.assign(base, base + n_media);
+  e->m_count.assign(count, count + n_media);
+  e->m_npole.assign(npole, npole + n_media);
+  long long ncoef = 0;
+  for (int m = 0; m < n_media; ++m) {
+    if (npole[m] < 0 || npole[m] > kMaxPoles)
+      return fail(e, PF_ERR_UNSUPPORTED, "at most %d poles per medium, got %d", kMaxPoles, npole[m]);
+    if (m > 0 && base[m] != base[m - 1] + count[m - 1])
+      return fail(e, PF_ERR_INVALID, "media compact ranges must be consecutive");
+    ncoef += 3LL * npole[m];
+  }
+  e->m_coef.assign(coef, coef + ncoef);
+  e->m_inv.assign(inv_eps, inv_eps + n_media);
+  e->m_ce.clear();
+  if (ce_m) e->m_ce.assign(ce_m, ce_m + n_media);
+  e->h_adeword.clear();
+  if (cell_word) e->h_adeword.assign(cell_word, cell_word + e->ncell);
+  return PF_OK;
+}
+
+int pf_set_sources(pf_engine* e, int n_src, const int32_t* comp, const int64_t* cell,
+                   const int32_t* wave_row, const double* amp, int n_wave, const double* wave) {
+  if (!e) return PF_ERR_INVALID;
+  if (e->finalized) return fail(e, PF_ERR_STATE, "pf_set_sources after pf_finalize");
+  for (int f = 0; f < 2; ++f) e->src[f] = SrcFamily();
+  e->n_wave = n_wave;
+  e->h_wave.assign(wave, wave + (size_t)n_wave * e->n_steps);
+  // group by (component, cell), keeping list order inside each group
+  for (int f = 0; f < 2; ++f) {
+    SrcFamily& s = e->src[f];
+    std::vector<std::pair<long long, int>> key;  // (comp*ncell + cell, source)
+    for (int q = 0; q < n_src; ++q) {
+      if (!valid_comp(comp[q])) return fail(e, PF_ERR_INVALID, "source %d: bad component %d", q, comp[q]);
+      if (cell[q] < 0 || cell[q] >= e->ncell) return fail(e, PF_ERR_INVALID, "source %d: cell out of range", q);
+      if (wave_row[q] < 0 || wave_row[q] >= n_wave) return fail(e, PF_ERR_INVALID, "source %d: bad waveform row", q);
+      if ((comp[q] >= 3) != (f == 1)) continue;
+      key.push_back({(long long)(comp[q] % 3) * e->ncell + cell[q], q});
+    }
+    std::stable_sort(key.begin(), key.end(),
+                     [](const std::pair<long long, int>& x, const std::pair<long long, int>& y) {
+                       return x.first < y.first;
+                     });
+    for (size_t q = 0; q < key.size(); ++q) {
+      if (q == 0 || key[q].first != key[q - 1].first) {
+        s.cell.push_back(key[q].first % e->ncell);
+        s.comp.push_back((int)(key[q].first / e->ncell));
+        s.start.push_back((int)s.wave_row.size());
+      }
+      s.wave_row.push_back(wave_row[key[q].second]);
+      s.amp.push_back(amp[key[q].second]);
+    }
+    s.start.push_back((int)s.wave_row.size());
+  }
+  return PF_OK;
+}
+
+int pf_add_dft(pf_engine* e, const int32_t start[3], const int32_t stop[3], const int32_t stride[3],
+               int comp_mask, int n_freq, int interval, const double* phase_e,
+               const double* phase_h, double dt, int* mon) {
+  if (!e) return PF_ERR_INVALID;
+  if (e->finalized) return fail(e, PF_ERR_STATE, "pf_add_dft after pf_finalize");
+  if (n_freq < 1 || interval < 1 || !(comp_mask & 63) || !phase_e || !phase_h)
+    return fail(e, PF_ERR_INVALID, "bad DFT monitor arguments");
+  const int dims[3] = {e->nx, e->ny, e->nz};
+  DftMon m;
+  m.r.ncell = 1;
+  for (int a = 0; a < 3; ++a) {
+    if (start[a] < 0 || stop[a] > dims[a] || stop[a] <= start[a] || stride[a] < 1)
+      return fail(e, PF_ERR_INVALID, "bad DFT region on axis %d", a);
+    m.r.start[a] = start[a];
+    m.r.stride[a] = stride[a];
+    m.r.count[a] = (stop[a] - start[a] + stride[a] - 1) / stride[a];
+    m.r.ncell *= m.r.count[a];
+  }
+  m.r.ncomp = 0;
+  for (int c = 0; c < 6; ++c)
+    if (comp_mask & (1 << c)) m.r.comps[m.r.ncomp++] = c;
+  m.n_freq = n_freq;
+  m.interval = interval;
+  m.dt = dt;
+  m.n_samples = e->n_steps > 0 ? (e->n_steps + interval - 1) / interval : 0;
+  m.h_ph_e.assign(phase_e, phase_e + m.n_samples * n_freq * 2);
+  m.h_ph_h.assign(phase_h, phase_h + m.n_samples * n_freq * 2);
+  e->dfts.push_back(std::move(m));
+  if (mon) *mon = (int)e->dfts.size() - 1;
+  return PF_OK;
+}
+
+int pf_add_flux(pf_engine* e, int axis, int idx, double dA, double dt, int* mon) {
+  if (!e) return PF_ERR_INVALID;
+  if (e->finalized) return fail(e, PF_ERR_STATE, "pf_add_flux after pf_finalize");
+  const int dims[3] = {e->nx, e->ny, e->nz};
+  if (axis < 0 || axis > 2 || idx < 0 || idx >= dims[axis])
+    return fail(e, PF_ERR_INVALID, "bad flux plane (axis %d, index %d)", axis, idx);
+  FluxMon f;
+  f.p.axis = axis;
+  f.p.idx = idx;
+  f.p.n0 = axis == 0 ? e->ny : e->nx;
+  f.p.n1 = axis == 2 ? e->ny : e->nz;
+  f.p.nblk = (int)(((long long)f.p.n0 * f.p.n1 + 255) / 256);
+  f.dA = dA;
+  f.dt = dt;
+  e->fluxes.push_back(f);
+  if (mon) *mon = (int)e->fluxes.size() - 1;
+  return PF_OK;
+}
+
+int pf_set_kernel(pf_engine* e, int kernel) {
+  if (!e) return PF_ERR_INVALID;
+  if (e->finalized) return fail(e, PF_ERR_STATE, "pf_set_kernel after pf_finalize");
+  if (kernel < PF_KERNEL_AUTO || kernel > PF_KERNEL_FUSED)
+    return fail(e, PF_ERR_INVALID, "unknown kernel %d", kernel);
+  e->kernel = kernel;
+  return PF_OK;
+}
+
+int pf_finalize(pf_engine* e) {
+  if (!e) return PF_ERR_INVALID;
+  if (e->finalized) return fail(e, PF_ERR_STATE, "pf_finalize called twice");
+  if (e->ce_mode < 0) return fail(e, PF_ERR_INVALID, "pf_set_ce was not called");
+  if (e->n_media > 0 && e->ce_mode == PF_CE_CELL3)
+    return fail(e, PF_ERR_UNSUPPORTED, "dispersive media with a three-component coefficient");
+  if (e->n_media > 0 && e->ce_mode == PF_CE_CELL1 && e->h_adeword.size() != (size_t)e->ncell)
+    return fail(e, PF_ERR_INVALID, "PF_CE_CELL1 with dispersive media needs cell_word");
+  const bool has_h_src = !e->src[1].cell.empty();
+  const bool fusable = fused_supported(e->nx, e->ny, e->nz) && !has_h_src;
+  if (e->kernel == PF_KERNEL_FUSED && !fusable)
+    return fail(e, PF_ERR_UNSUPPORTED, "the fused kernel needs a 3D grid without H-family sources");
+  e->fused = (e->kernel == PF_KERNEL_FUSED) || (e->kernel == PF_KERNEL_AUTO && fusable);
+  int rc = e->rb == 4 ? finalize_typed<float>(e) : finalize_typed<double>(e);
+  if (rc) return rc;
+  // host staging no longer needed
+  for (int c = 0; c < 3; ++c) std::vector<char>().swap(e->h_ce[c]);
+  std::vector<uint32_t>().swap(e->h_word);
+  std::vector<uint32_t>().swap(e->h_adeword);
+  e->finalized = true;
+  return PF_OK;
+}
+
+int pf_advance(pf_engine* e, int64_t step0, int64_t n_sub) {
+  if (!e) return PF_ERR_INVALID;
+  if (!e->finalized) return fail(e, PF_ERR_STATE, "pf_advance before pf_finalize");
+  if (step0 != e->step)
+    return fail(e, PF_ERR_INVALID, "pf_advance(step0=%lld) but the engine is at step %lld",
+                (long long)step0, e->step);
+  if (n_sub < 0 || e->step + n_sub > e->n_steps)
+    return fail(e, PF_ERR_INVALID, "advance past n_steps (%lld)", e->n_steps);
+  PF_CUDA(e, cudaSetDevice(e->device));
+  return e->rb == 4 ? advance_typed<float>(e, n_sub) : advance_typed<double>(e, n_sub);
+}
+
+int pf_read_field(pf_engine* e, int comp, void* dst) {
+  if (!e || !dst) return PF_ERR_INVALID;
+  if (!e->finalized) return fail(e, PF_ERR_STATE, "pf_read_field before pf_finalize");
+  if (!valid_comp(comp)) return fail(e, PF_ERR_INVALID, "bad component %d", comp);
+  void* src = comp < 3 ? e->E[e->cur][comp] : e->H[e->cur][comp - 3];
+  PF_CUDA(e, cudaMemcpyAsync(dst, src, (size_t)e->ncell * e->rb, cudaMemcpyDeviceToHost, e->stream));
+  PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  return PF_OK;
+}
+
+int pf_read_dft(pf_engine* e, int mon, int comp, double* dst) {
+  if (!e || !dst) return PF_ERR_INVALID;
+  if (!e->finalized) return fail(e, PF_ERR_STATE, "pf_read_dft before pf_finalize");
+  if (mon < 0 || mon >= (int)e->dfts.size()) return fail(e, PF_ERR_INVALID, "bad DFT monitor %d", mon);
+  DftMon& m = e->dfts[mon];
+  int qc = -1;
+  for (int q = 0; q < m.r.ncomp; ++q)
+    if (m.r.comps[q] == comp) qc = q;
+  if (qc < 0) return fail(e, PF_ERR_INVALID, "component %d not recorded by DFT monitor %d", comp, mon);
+  int rc = e->rb == 4 ? flush_monitors<float>(e) : flush_monitors<double>(e);
+  if (rc) return rc;
+  const size_t per = (size_t)m.n_freq * m.r.ncell * 16;
+  PF_CUDA(e, cudaMemcpyAsync(dst, (const char*)m.acc + per * qc, per, cudaMemcpyDeviceToHost, e->stream));
+  PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  return PF_OK;
+}
+
+int pf_read_flux(pf_engine* e, int mon, double* dst) {
+  if (!e || !dst) return PF_ERR_INVALID;
+  if (!e->finalized) return fail(e, PF_ERR_STATE, "pf_read_flux before pf_finalize");
+  if (mon < 0 || mon >= (int)e->fluxes.size()) return fail(e, PF_ERR_INVALID, "bad flux monitor %d", mon);
+  int rc = e->rb == 4 ? flush_monitors<float>(e) : flush_monitors<double>(e);
+  if (rc) return rc;
+  PF_CUDA(e, cudaMemcpyAsync(dst, e->fluxes[mon].acc, 8, cudaMemcpyDeviceToHost, e->stream));
+  PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  return PF_OK;
+}
+
+int pf_step(const pf_engine* e, int64_t* step) {
+  if (!e || !step) return PF_ERR_INVALID;
+  *step = e->step;
+  return PF_OK;
+}
+
+int pf_check_finite(pf_engine* e) {
+  if (!e) return PF_ERR_INVALID;
+  if (!e->finalized) return fail(e, PF_ERR_STATE, "pf_check_finite before pf_finalize");
+  int* flag = e->flag;
+  PF_CUDA(e, cudaMemsetAsync(flag, 0, sizeof(int), e->stream));
+  for (int c = 0; c < 6; ++c) {
+    const void* f = c < 3 ? e->E[e->cur][c] : e->H[e->cur][c - 3];
+    if (e->rb == 4)
+      k_nonfinite<float><<<592, 256, 0, e->stream>>>((const float*)f, e->ncell, flag);
+    else
+      k_nonfinite<double><<<592, 256, 0, e->stream>>>((const double*)f, e->ncell, flag);
+  }
+  int h = 0;
+  PF_CUDA(e, cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  return h ? fail(e, PF_ERR_NONFINITE, "non-finite field value at step %lld", e->step) : PF_OK;
+}
+
+int pf_stream(const pf_engine* e, void** stream) {
+  if (!e || !stream) return PF_ERR_INVALID;
+  *stream = (void*)e->stream;
+  return PF_OK;
+}
+
+int pf_set_profiling(pf_engine* e, int on) {
+  if (!e) return PF_ERR_INVALID;
+  e->profiling = on != 0;
+  return PF_OK;
+}
+
+int pf_read_profile(pf_engine* e, int64_t launches[4], double ms[4], int reset) {
+  if (!e) return PF_ERR_INVALID;
+  PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  collect_profile(e);
+  for (int k = 0; k < 4; ++k) {
+    if (launches) launches[k] = e->launches[k];
+    if (ms) ms[k] = e->prof_ms[k];
+    if (reset) {
+      e->launches[k] = 0;
+      e->prof_ms[k] = 0.0;
+    }
+  }
+  return PF_OK;
+}
+
+int pf_device_bytes(const pf_engine* e, int64_t* bytes) {
+  if (!e || !bytes) return PF_ERR_INVALID;
+  *bytes = (int64_t)e->dev_bytes;
+  return PF_OK;
+}
+
+void pf_destroy(pf_engine* e) {
+  if (!e) return;
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  for (void* p : e->allocs) cudaFree(p);
+  for (cudaEvent_t ev : e->ev_pool) cudaEventDestroy(ev);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+}  // extern "C"

@@ -1,0 +1,51 @@
+"""The CPU oracle against the reference's own outputs (tests/golden).
+
+These pin the oracle: on every golden scene it must reproduce the reference
+NumPy run (ngpaladi/photonfdtd src/photonfdtd/simulation.py:910-1436) to the
+last bit, which is what lets the GPU parity tests use it as the checker on a
+machine where the reference is absent.
+"""
+import numpy as np
+import pytest
+
+import photonfdtd_b200 as pf
+import scenes
+from golden_util import compare, load
+from oracle import run_oracle
+
+FAST = [n for n in scenes.SCENES if n not in ("ade3d_f32",)]
+
+
+@pytest.mark.parametrize("name", FAST)
+def test_oracle_matches_reference(name):
+    sim = scenes.build(name, pf)
+    _, meta = load(name)
+    assert sim.dt == meta["dt"] and sim.n_steps == meta["n_steps"]
+    res = run_oracle(sim)
+    for k, (rmax, rl2) in compare(res, name).items():
+        assert rmax == 0.0, f"{name} {k}: oracle differs from the reference ({rmax:.3e})"
+
+
+@pytest.mark.slow
+def test_oracle_matches_reference_ade3d():
+    """The reduced config-3 scene (64^3, 3000 steps, Drude + 2-pole Lorentz +
+    dielectric blocks, six flux planes, DFT): about 90 s on one core."""
+    sim = scenes.build("ade3d_f32", pf)
+    res = run_oracle(sim)
+    for k, (rmax, rl2) in compare(res, "ade3d_f32").items():
+        assert rmax == 0.0, f"ade3d {k}: {rmax:.3e}"
+
+
+def test_planted_error_is_caught():
+    """A one-ulp change in one CPML coefficient of the oracle must show up in
+    the comparison (the check is not vacuous)."""
+    import oracle.fdtd_oracle as O
+    sim = scenes.build("tm2d_f64", pf)
+    run = O.OracleRun(sim)
+    name, reg, k_arr, k_sc, is_e, terms = run.updates[0]
+    sl, bb, cc, psi = terms[0][4][0]
+    bb.flat[0] = np.nextafter(bb.flat[0], 2.0)
+    run.advance(run.n_steps)
+    res = run.result()
+    worst = max(v[0] for v in compare(res, "tm2d_f64").values())
+    assert worst > 0.0
