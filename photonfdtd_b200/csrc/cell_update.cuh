@@ -1,0 +1,244 @@
+// cell_update.cuh - per-cell curl updates shared by the split and fused kernels.
+//
+// Each function updates one field component at cell (i, j, k) from its
+// neighbour values, following src/photonfdtd/simulation.py:1252-1309 exactly
+// (see curl_update in kernels_split.cuh for the operation order), and applies
+// the reference's loop extents: forward differences (H) stop one cell short
+// of the high face, backward differences (E) start at index 1, and a term on
+// a collapsed axis is absent. Neighbour values outside those extents are
+// never read. write_psi = false computes a halo cell's value without storing
+// its CPML state (the owning tile stores it).
+#pragma once
+
+#include "common.cuh"
+
+namespace pfb {
+
+template <typename T>
+__device__ __forceinline__ T curl_term(T f, T k, bool hasA, T dA, bool hasB, T dB, long long qA,
+                                       T bA, T cA, const T* psiAin, T* psiAout, long long qB, T bB,
+                                       T cB, const T* psiBin, T* psiBout, bool write_psi) {
+  T curl = hasA ? (hasB ? sub_rn(dA, dB) : dA) : -dB;
+  f = add_rn(f, mul_rn(curl, k));
+  if (hasA && qA >= 0) {
+    T psi = add_rn(mul_rn(bA, psiAin[qA]), mul_rn(cA, dA));
+    if (write_psi) psiAout[qA] = psi;
+    f = add_rn(f, mul_rn(k, psi));
+  }
+  if (hasB && qB >= 0) {
+    T psi = add_rn(mul_rn(bB, psiBin[qB]), mul_rn(cB, dB));
+    if (write_psi) psiBout[qB] = psi;
+    f = add_rn(f, mul_rn(-k, psi));
+  }
+  return f;
+}
+
+// Compact psi index of a term on axis `ax` at (i, j, k), or -1 (bulk).
+template <typename T>
+__device__ __forceinline__ long long psi_index(const int* map, const int* np, int ax, int i, int j,
+                                               int k, int ny, int nz) {
+  if (ax == 0) {
+    const int m = map[i];
+    return m < 0 ? -1 : ((long long)m * ny + j) * nz + k;
+  }
+  if (ax == 1) {
+    const int m = map[j];
+    return m < 0 ? -1 : ((long long)i * np[1] + m) * nz + k;
+  }
+  const int m = map[k];
+  return m < 0 ? -1 : ((long long)i * ny + j) * np[2] + m;
+}
+
+// ---- H components (forward differences of E^n) ----------------------------
+// Hx: +dEz/dy - dEy/dz
+template <typename T>
+__device__ __forceinline__ T upd_hx(const StepArgs<T>& a, int i, int j, int k, T h, T ez_jp,
+                                    T ez, T ey_kp, T ey, bool write_psi) {
+  const bool ry = a.ny > 1, rz = a.nz > 1;
+  if (!((!ry || j < a.ny - 1) && (!rz || k < a.nz - 1) && (ry || rz))) return h;
+  T dA = T(0), dB = T(0);
+  long long qA = -1, qB = -1;
+  if (ry) {
+    dA = div_rn(sub_rn(ez_jp, ez), a.dy);
+    qA = psi_index<T>(a.maph[1], a.nph, 1, i, j, k, a.ny, a.nz);
+  }
+  if (rz) {
+    dB = div_rn(sub_rn(ey_kp, ey), a.dz);
+    qB = psi_index<T>(a.maph[2], a.nph, 2, i, j, k, a.ny, a.nz);
+  }
+  return curl_term<T>(h, -a.ch, ry, dA, rz, dB, qA, ry ? a.bh[1][j] : T(0), ry ? a.cph[1][j] : T(0),
+                      a.psiHin[0], a.psiHout[0], qB, rz ? a.bh[2][k] : T(0),
+                      rz ? a.cph[2][k] : T(0), a.psiHin[1], a.psiHout[1], write_psi);
+}
+
+// Hy: +dEx/dz - dEz/dx
+template <typename T>
+__device__ __forceinline__ T upd_hy(const StepArgs<T>& a, int i, int j, int k, T h, T ex_kp,
+                                    T ex, T ez_ip, T ez, bool write_psi) {
+  const bool rz = a.nz > 1, rx = a.nx > 1;
+  if (!((!rz || k < a.nz - 1) && (!rx || i < a.nx - 1) && (rz || rx))) return h;
+  T dA = T(0), dB = T(0);
+  long long qA = -1, qB = -1;
+  if (rz) {
+    dA = div_rn(sub_rn(ex_kp, ex), a.dz);
+    qA = psi_index<T>(a.maph[2], a.nph, 2, i, j, k, a.ny, a.nz);
+  }
+  if (rx) {
+    dB = div_rn(sub_rn(ez_ip, ez), a.dx);
+    qB = psi_index<T>(a.maph[0], a.nph, 0, i, j, k, a.ny, a.nz);
+  }
+  return curl_term<T>(h, -a.ch, rz, dA, rx, dB, qA, rz ? a.bh[2][k] : T(0), rz ? a.cph[2][k] : T(0),
+                      a.psiHin[2], a.psiHout[2], qB, rx ? a.bh[0][i] : T(0),
+                      rx ? a.cph[0][i] : T(0), a.psiHin[3], a.psiHout[3], write_psi);
+}
+
+// Hz: +dEy/dx - dEx/dy
+template <typename T>
+__device__ __forceinline__ T upd_hz(const StepArgs<T>& a, int i, int j, int k, T h, T ey_ip,
+                                    T ey, T ex_jp, T ex, bool write_psi) {
+  const bool rx = a.nx > 1, ry = a.ny > 1;
+  if (!((!rx || i < a.nx - 1) && (!ry || j < a.ny - 1) && (rx || ry))) return h;
+  T dA = T(0), dB = T(0);
+  long long qA = -1, qB = -1;
+  if (rx) {
+    dA = div_rn(sub_rn(ey_ip, ey), a.dx);
+    qA = psi_index<T>(a.maph[0], a.nph, 0, i, j, k, a.ny, a.nz);
+  }
+  if (ry) {
+    dB = div_rn(sub_rn(ex_jp, ex), a.dy);
+    qB = psi_index<T>(a.maph[1], a.nph, 1, i, j, k, a.ny, a.nz);
+  }
+  return curl_term<T>(h, -a.ch, rx, dA, ry, dB, qA, rx ? a.bh[0][i] : T(0), rx ? a.cph[0][i] : T(0),
+                      a.psiHin[4], a.psiHout[4], qB, ry ? a.bh[1][j] : T(0),
+                      ry ? a.cph[1][j] : T(0), a.psiHin[5], a.psiHout[5], write_psi);
+}
+
+// ---- E components (backward differences of H^{n+1/2}) ----------------------
+// Ex: +dHz/dy - dHy/dz
+template <typename T>
+__device__ __forceinline__ T upd_ex(const StepArgs<T>& a, int i, int j, int k, T e, T K, T hz,
+                                    T hz_jm, T hy, T hy_km) {
+  const bool ry = a.ny > 1, rz = a.nz > 1;
+  if (!((!ry || j >= 1) && (!rz || k >= 1) && (ry || rz))) return e;
+  T dA = T(0), dB = T(0);
+  long long qA = -1, qB = -1;
+  if (ry) {
+    dA = div_rn(sub_rn(hz, hz_jm), a.dy);
+    qA = psi_index<T>(a.mape[1], a.npe, 1, i, j, k, a.ny, a.nz);
+  }
+  if (rz) {
+    dB = div_rn(sub_rn(hy, hy_km), a.dz);
+    qB = psi_index<T>(a.mape[2], a.npe, 2, i, j, k, a.ny, a.nz);
+  }
+  return curl_term<T>(e, K, ry, dA, rz, dB, qA, ry ? a.be[1][j] : T(0), ry ? a.cpe[1][j] : T(0),
+                      a.psiE[0], a.psiE[0], qB, rz ? a.be[2][k] : T(0), rz ? a.cpe[2][k] : T(0),
+                      a.psiE[1], a.psiE[1], true);
+}
+
+// Ey: +dHx/dz - dHz/dx
+template <typename T>
+__device__ __forceinline__ T upd_ey(const StepArgs<T>& a, int i, int j, int k, T e, T K, T hx,
+                                    T hx_km, T hz, T hz_im) {
+  const bool rz = a.nz > 1, rx = a.nx > 1;
+  if (!((!rz || k >= 1) && (!rx || i >= 1) && (rz || rx))) return e;
+  T dA = T(0), dB = T(0);
+  long long qA = -1, qB = -1;
+  if (rz) {
+    dA = div_rn(sub_rn(hx, hx_km), a.dz);
+    qA = psi_index<T>(a.mape[2], a.npe, 2, i, j, k, a.ny, a.nz);
+  }
+  if (rx) {
+    dB = div_rn(sub_rn(hz, hz_im), a.dx);
+    qB = psi_index<T>(a.mape[0], a.npe, 0, i, j, k, a.ny, a.nz);
+  }
+  return curl_term<T>(e, K, rz, dA, rx, dB, qA, rz ? a.be[2][k] : T(0), rz ? a.cpe[2][k] : T(0),
+                      a.psiE[2], a.psiE[2], qB, rx ? a.be[0][i] : T(0), rx ? a.cpe[0][i] : T(0),
+                      a.psiE[3], a.psiE[3], true);
+}
+
+// Ez: +dHy/dx - dHx/dy
+template <typename T>
+__device__ __forceinline__ T upd_ez(const StepArgs<T>& a, int i, int j, int k, T e, T K, T hy,
+                                    T hy_im, T hx, T hx_jm) {
+  const bool rx = a.nx > 1, ry = a.ny > 1;
+  if (!((!rx || i >= 1) && (!ry || j >= 1) && (rx || ry))) return e;
+  T dA = T(0), dB = T(0);
+  long long qA = -1, qB = -1;
+  if (rx) {
+    dA = div_rn(sub_rn(hy, hy_im), a.dx);
+    qA = psi_index<T>(a.mape[0], a.npe, 0, i, j, k, a.ny, a.nz);
+  }
+  if (ry) {
+    dB = div_rn(sub_rn(hx, hx_jm), a.dy);
+    qB = psi_index<T>(a.mape[1], a.npe, 1, i, j, k, a.ny, a.nz);
+  }
+  return curl_term<T>(e, K, rx, dA, ry, dB, qA, rx ? a.be[0][i] : T(0), rx ? a.cpe[0][i] : T(0),
+                      a.psiE[4], a.psiE[4], qB, ry ? a.be[1][j] : T(0), ry ? a.cpe[1][j] : T(0),
+                      a.psiE[5], a.psiE[5], true);
+}
+
+// Locate the medium of compact dispersive index g (media sorted by base).
+template <typename T>
+__device__ __forceinline__ int find_medium(const MediumT<T>* media, int n, long long g) {
+  int m = 0;
+  for (int q = 1; q < n; ++q)
+    if (g >= media[q].base) m = q;
+  return m;
+}
+
+// ADE polarisation update and E correction for one dispersive cell
+// (simulation.py:645-669): P^{n+1} = a P^n + b P^{n-1} + c E^n per pole and
+// component, E -= inv * sum_p (P^{n+1} - P^n). P^{n+1} overwrites P^{n-1}.
+template <typename T>
+__device__ __forceinline__ void ade_apply(const StepArgs<T>& a, long long g, const T en[3],
+                                          T e[3]) {
+  const int m = find_medium(a.media, a.n_media, g);
+  const MediumT<T>& M = a.media[m];
+  const long long loc = g - M.base, cnt = M.count;
+  T* P = a.P + M.poff;
+  const int np = M.npole;
+  const int lc = a.lvl, lp = a.lvl ^ 1;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    T delta = T(0);
+    for (int p = 0; p < np; ++p) {
+      const long long ic = ((long long)(lc * np + p) * 3 + c) * cnt + loc;
+      const long long ip = ((long long)(lp * np + p) * 3 + c) * cnt + loc;
+      const T pc = P[ic], pp = P[ip];
+      const T pn = add_rn(add_rn(mul_rn(M.a[p], pc), mul_rn(M.b[p], pp)), mul_rn(M.c[p], en[c]));
+      P[ip] = pn;
+      const T inc = sub_rn(pn, pc);
+      delta = p == 0 ? inc : add_rn(delta, inc);
+    }
+    if (np > 0) e[c] = sub_rn(e[c], mul_rn(M.inv, delta));
+  }
+}
+
+// E-update coefficients of one cell and its compact dispersive index (-1 if
+// the cell is not dispersive).
+template <typename T, int CE, bool ADE>
+__device__ __forceinline__ void cell_coeffs(const StepArgs<T>& a, long long id, T K[3],
+                                            long long& g) {
+  g = -1;
+  if (CE == kCeCell1) {
+    K[0] = K[1] = K[2] = a.ce[0][id];
+  } else if (CE == kCeCell3) {
+    K[0] = a.ce[0][id];
+    K[1] = a.ce[1][id];
+    K[2] = a.ce[2][id];
+  } else {
+    const uint32_t w = a.word[id];
+    if (ADE && (w & kDispersiveBit)) {
+      g = (long long)(w & ~kDispersiveBit);
+      K[0] = K[1] = K[2] = a.media[find_medium(a.media, a.n_media, g)].ce;
+    } else {
+      K[0] = K[1] = K[2] = a.table[w & ~kDispersiveBit];
+    }
+  }
+  if (ADE && CE == kCeCell1) {
+    const uint32_t w = a.adeword[id];
+    if (w) g = (long long)w - 1;
+  }
+}
+
+}  // namespace pfb

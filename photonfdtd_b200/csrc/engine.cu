@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -115,6 +116,8 @@ struct pf_engine {
   double* wave = nullptr;
   int* flag = nullptr;
   bool fused = false;
+  int fused_ty = 8;      // fused tile height (8 or 16), env PFB200_FUSED_TY
+  int fused_chunks = 0;  // x chunks per column (0 = auto), env PFB200_XCHUNKS
 
   // launch accounting (pf_read_profile)
   long long launches[4] = {};
@@ -466,7 +469,8 @@ int advance_typed(pf_engine* e, long long n_sub) {
       int rc;
       {
         LaunchScope ls(e, 0);
-        rc = launch_fused<T>(e->stream, a, e->ce_mode, e->n_media > 0);
+        rc = launch_fused<T>(e->stream, a, e->ce_mode, e->n_media > 0, e->fused_ty,
+                             e->fused_chunks);
       }
       if (rc) return fail(e, PF_ERR_UNSUPPORTED, "fused kernel does not cover this case");
       // sources of the fused path are injected after its single pass: an H
@@ -729,6 +733,16 @@ int pf_finalize(pf_engine* e) {
   if (e->kernel == PF_KERNEL_FUSED && !fusable)
     return fail(e, PF_ERR_UNSUPPORTED, "the fused kernel needs a 3D grid without H-family sources");
   e->fused = (e->kernel == PF_KERNEL_FUSED) || (e->kernel == PF_KERNEL_AUTO && fusable);
+  if (e->fused) {
+    if (const char* v = getenv("PFB200_FUSED_TY")) e->fused_ty = atoi(v) == 16 ? 16 : 8;
+    const long long tiles = (long long)((e->nz + 31) / 32) * ((e->ny + e->fused_ty - 1) / e->fused_ty);
+    // about one resident wave of blocks (148 SMs x 1024 threads), at least
+    // 8 planes per chunk
+    int nch = (int)std::max<long long>(1, (148LL * 1024 / (32 * e->fused_ty) + tiles / 2) / tiles);
+    nch = std::min(nch, std::max(1, e->nx / 8));
+    if (const char* v = getenv("PFB200_XCHUNKS")) nch = std::max(1, atoi(v));
+    e->fused_chunks = nch;
+  }
   int rc = e->rb == 4 ? finalize_typed<float>(e) : finalize_typed<double>(e);
   if (rc) return rc;
   // host staging no longer needed
