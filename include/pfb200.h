@@ -46,7 +46,7 @@ extern "C" {
 #define PF_CE_TABLE 2 /* per-cell uint32 word indexing a coefficient table */
 
 /* Stepping kernels (pf_set_kernel). */
-#define PF_KERNEL_AUTO 0  /* fused single-pass kernel where it applies     */
+#define PF_KERNEL_AUTO 0  /* the faster path for the grid (split on B200) */
 #define PF_KERNEL_SPLIT 1 /* separate H and E passes, one thread per cell  */
 #define PF_KERNEL_FUSED 2 /* require the fused H+E pass (3D only)          */
 
@@ -89,18 +89,16 @@ int pf_set_cpml(pf_engine *eng, int axis, const void *b_e, const void *c_e,
                 const void *b_h, const void *c_h);
 
 /* Dispersive (ADE) media (simulation.py:572-669). n_media <= 16.
- *  cell_word: PF_CE_TABLE mode: NULL (the ce word carries the dispersive
- *    index); PF_CE_CELL1 mode: nx*ny*nz uint32, 0 = non-dispersive, else
- *    1 + compact index.
- *  The compact index of a dispersive cell runs over media in order: medium m
- *  owns [base[m], base[m] + count[m]); within a medium cells are in C order.
+ *  A dispersive cell's word is 0x80000000 | (m << 27) | loc: medium m, and
+ *  loc = its rank among medium m's cells in C order (loc < count[m] <= 2^27).
+ *  cell_word: PF_CE_TABLE mode: NULL (the ce word carries it); PF_CE_CELL1
+ *    mode: nx*ny*nz uint32, 0 for a plain cell.
  *  npole[m] <= 8; coef holds, per medium, per pole, (a, b, c) as doubles;
  *  inv_eps[m] = 1/(eps0*eps_inf); ce_m[m] = the medium's coefficient in table
  *  mode (ignored otherwise). */
-int pf_set_ade(pf_engine *eng, int n_media, const int64_t *base,
-               const int64_t *count, const int32_t *npole, const double *coef,
-               const double *inv_eps, const double *ce_m,
-               const uint32_t *cell_word);
+int pf_set_ade(pf_engine *eng, int n_media, const int64_t *count,
+               const int32_t *npole, const double *coef, const double *inv_eps,
+               const double *ce_m, const uint32_t *cell_word);
 
 /* Soft point sources (simulation.py:1367-1390; rustbackend.py:151-166).
  * n_src entries in the reference's source order: comp (0..5), flat cell
@@ -173,6 +171,11 @@ int pf_stream(const pf_engine *eng, void **stream);
  * so time work with it off. */
 int pf_set_profiling(pf_engine *eng, int on);
 int pf_read_profile(pf_engine *eng, int64_t launches[4], double ms[4], int reset);
+
+/* Engine configuration as "key=value" pairs separated by spaces (kernel
+ * path, tile shape, x chunks, reciprocal-division axes, coefficient mode,
+ * media), written NUL-terminated into buf (at most len bytes). */
+int pf_info(const pf_engine *eng, char *buf, int len);
 
 /* Device bytes held by the engine. */
 int pf_device_bytes(const pf_engine *eng, int64_t *bytes);

@@ -43,7 +43,7 @@ SIGNATURES = {
                             C.POINTER(_vp)]),
     "pf_set_ce": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _pu32, C.c_int, _pdbl]),
     "pf_set_cpml": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp]),
-    "pf_set_ade": (C.c_int, [_vp, C.c_int, _pi64, _pi64, _pi32, _pdbl, _pdbl, _pdbl, _pu32]),
+    "pf_set_ade": (C.c_int, [_vp, C.c_int, _pi64, _pi32, _pdbl, _pdbl, _pdbl, _pu32]),
     "pf_set_sources": (C.c_int, [_vp, C.c_int, _pi32, _pi64, _pi32, _pdbl, C.c_int, _pdbl]),
     "pf_add_dft": (C.c_int, [_vp, _pi32, _pi32, _pi32, C.c_int, C.c_int, C.c_int, _pdbl, _pdbl,
                              _dbl, C.POINTER(C.c_int)]),
@@ -60,6 +60,7 @@ SIGNATURES = {
     "pf_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "pf_set_profiling": (C.c_int, [_vp, C.c_int]),
     "pf_read_profile": (C.c_int, [_vp, _pi64, _pdbl, C.c_int]),
+    "pf_info": (C.c_int, [_vp, C.c_char_p, C.c_int]),
     "pf_destroy": (None, [_vp]),
 }
 

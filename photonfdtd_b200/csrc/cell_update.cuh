@@ -33,6 +33,13 @@ __device__ __forceinline__ T curl_term(T f, T k, bool hasA, T dA, bool hasB, T d
   return f;
 }
 
+// Bulk curl update: f + K * (dA - dB), the reference's bulk term with no
+// CPML correction (simulation.py:1284-1288); curl_term with no psi.
+template <typename T>
+__device__ __forceinline__ T bulk(T f, T k, T dA, T dB) {
+  return add_rn(f, mul_rn(sub_rn(dA, dB), k));
+}
+
 // Compact psi index of a term on axis `ax` at (i, j, k), or -1 (bulk).
 template <typename T>
 __device__ __forceinline__ long long psi_index(const int* map, const int* np, int ax, int i, int j,
@@ -59,11 +66,11 @@ __device__ __forceinline__ T upd_hx(const StepArgs<T>& a, int i, int j, int k, T
   T dA = T(0), dB = T(0);
   long long qA = -1, qB = -1;
   if (ry) {
-    dA = div_rn(sub_rn(ez_jp, ez), a.dy);
+    dA = qdiv(sub_rn(ez_jp, ez), a.dy, a.rdy, a.fdy);
     qA = psi_index<T>(a.maph[1], a.nph, 1, i, j, k, a.ny, a.nz);
   }
   if (rz) {
-    dB = div_rn(sub_rn(ey_kp, ey), a.dz);
+    dB = qdiv(sub_rn(ey_kp, ey), a.dz, a.rdz, a.fdz);
     qB = psi_index<T>(a.maph[2], a.nph, 2, i, j, k, a.ny, a.nz);
   }
   return curl_term<T>(h, -a.ch, ry, dA, rz, dB, qA, ry ? a.bh[1][j] : T(0), ry ? a.cph[1][j] : T(0),
@@ -80,11 +87,11 @@ __device__ __forceinline__ T upd_hy(const StepArgs<T>& a, int i, int j, int k, T
   T dA = T(0), dB = T(0);
   long long qA = -1, qB = -1;
   if (rz) {
-    dA = div_rn(sub_rn(ex_kp, ex), a.dz);
+    dA = qdiv(sub_rn(ex_kp, ex), a.dz, a.rdz, a.fdz);
     qA = psi_index<T>(a.maph[2], a.nph, 2, i, j, k, a.ny, a.nz);
   }
   if (rx) {
-    dB = div_rn(sub_rn(ez_ip, ez), a.dx);
+    dB = qdiv(sub_rn(ez_ip, ez), a.dx, a.rdx, a.fdx);
     qB = psi_index<T>(a.maph[0], a.nph, 0, i, j, k, a.ny, a.nz);
   }
   return curl_term<T>(h, -a.ch, rz, dA, rx, dB, qA, rz ? a.bh[2][k] : T(0), rz ? a.cph[2][k] : T(0),
@@ -101,11 +108,11 @@ __device__ __forceinline__ T upd_hz(const StepArgs<T>& a, int i, int j, int k, T
   T dA = T(0), dB = T(0);
   long long qA = -1, qB = -1;
   if (rx) {
-    dA = div_rn(sub_rn(ey_ip, ey), a.dx);
+    dA = qdiv(sub_rn(ey_ip, ey), a.dx, a.rdx, a.fdx);
     qA = psi_index<T>(a.maph[0], a.nph, 0, i, j, k, a.ny, a.nz);
   }
   if (ry) {
-    dB = div_rn(sub_rn(ex_jp, ex), a.dy);
+    dB = qdiv(sub_rn(ex_jp, ex), a.dy, a.rdy, a.fdy);
     qB = psi_index<T>(a.maph[1], a.nph, 1, i, j, k, a.ny, a.nz);
   }
   return curl_term<T>(h, -a.ch, rx, dA, ry, dB, qA, rx ? a.bh[0][i] : T(0), rx ? a.cph[0][i] : T(0),
@@ -123,11 +130,11 @@ __device__ __forceinline__ T upd_ex(const StepArgs<T>& a, int i, int j, int k, T
   T dA = T(0), dB = T(0);
   long long qA = -1, qB = -1;
   if (ry) {
-    dA = div_rn(sub_rn(hz, hz_jm), a.dy);
+    dA = qdiv(sub_rn(hz, hz_jm), a.dy, a.rdy, a.fdy);
     qA = psi_index<T>(a.mape[1], a.npe, 1, i, j, k, a.ny, a.nz);
   }
   if (rz) {
-    dB = div_rn(sub_rn(hy, hy_km), a.dz);
+    dB = qdiv(sub_rn(hy, hy_km), a.dz, a.rdz, a.fdz);
     qB = psi_index<T>(a.mape[2], a.npe, 2, i, j, k, a.ny, a.nz);
   }
   return curl_term<T>(e, K, ry, dA, rz, dB, qA, ry ? a.be[1][j] : T(0), ry ? a.cpe[1][j] : T(0),
@@ -144,11 +151,11 @@ __device__ __forceinline__ T upd_ey(const StepArgs<T>& a, int i, int j, int k, T
   T dA = T(0), dB = T(0);
   long long qA = -1, qB = -1;
   if (rz) {
-    dA = div_rn(sub_rn(hx, hx_km), a.dz);
+    dA = qdiv(sub_rn(hx, hx_km), a.dz, a.rdz, a.fdz);
     qA = psi_index<T>(a.mape[2], a.npe, 2, i, j, k, a.ny, a.nz);
   }
   if (rx) {
-    dB = div_rn(sub_rn(hz, hz_im), a.dx);
+    dB = qdiv(sub_rn(hz, hz_im), a.dx, a.rdx, a.fdx);
     qB = psi_index<T>(a.mape[0], a.npe, 0, i, j, k, a.ny, a.nz);
   }
   return curl_term<T>(e, K, rz, dA, rx, dB, qA, rz ? a.be[2][k] : T(0), rz ? a.cpe[2][k] : T(0),
@@ -165,11 +172,11 @@ __device__ __forceinline__ T upd_ez(const StepArgs<T>& a, int i, int j, int k, T
   T dA = T(0), dB = T(0);
   long long qA = -1, qB = -1;
   if (rx) {
-    dA = div_rn(sub_rn(hy, hy_im), a.dx);
+    dA = qdiv(sub_rn(hy, hy_im), a.dx, a.rdx, a.fdx);
     qA = psi_index<T>(a.mape[0], a.npe, 0, i, j, k, a.ny, a.nz);
   }
   if (ry) {
-    dB = div_rn(sub_rn(hx, hx_jm), a.dy);
+    dB = qdiv(sub_rn(hx, hx_jm), a.dy, a.rdy, a.fdy);
     qB = psi_index<T>(a.mape[1], a.npe, 1, i, j, k, a.ny, a.nz);
   }
   return curl_term<T>(e, K, rx, dA, ry, dB, qA, rx ? a.be[0][i] : T(0), rx ? a.cpe[0][i] : T(0),
@@ -177,36 +184,115 @@ __device__ __forceinline__ T upd_ez(const StepArgs<T>& a, int i, int j, int k, T
                       a.psiE[5], a.psiE[5], true);
 }
 
-// Locate the medium of compact dispersive index g (media sorted by base).
+// Vector load/store of N consecutive reals (N*sizeof(T) a multiple of the
+// vector width, pointer aligned to it).
+template <typename T, int N>
+__device__ __forceinline__ void ldv(const T* p, T* o) {
+  if constexpr (sizeof(T) == 4 && N % 4 == 0) {
+#pragma unroll
+    for (int q = 0; q < N / 4; ++q) {
+      const float4 v = reinterpret_cast<const float4*>(p)[q];
+      o[4 * q] = v.x; o[4 * q + 1] = v.y; o[4 * q + 2] = v.z; o[4 * q + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < N / 2; ++q) {
+      if constexpr (sizeof(T) == 4) {
+        const float2 v = reinterpret_cast<const float2*>(p)[q];
+        o[2 * q] = v.x; o[2 * q + 1] = v.y;
+      } else {
+        const double2 v = reinterpret_cast<const double2*>(p)[q];
+        o[2 * q] = v.x; o[2 * q + 1] = v.y;
+      }
+    }
+  }
+}
+template <typename T, int N>
+__device__ __forceinline__ void stv(T* p, const T* o) {
+#pragma unroll
+  for (int q = 0; q < N / 2; ++q) {
+    if constexpr (sizeof(T) == 4) {
+      reinterpret_cast<float2*>(p)[q] = make_float2(o[2 * q], o[2 * q + 1]);
+    } else {
+      reinterpret_cast<double2*>(p)[q] = make_double2(o[2 * q], o[2 * q + 1]);
+    }
+  }
+}
+
+// Polarisation record of one dispersive cell, loaded ahead of its use.
 template <typename T>
-__device__ __forceinline__ int find_medium(const MediumT<T>* media, int n, long long g) {
-  int m = 0;
-  for (int q = 1; q < n; ++q)
-    if (g >= media[q].base) m = q;
-  return m;
+struct AdeRec {
+  T v[12];   // [level][pole][component] for npole <= 2
+  int m;     // medium
+  uint32_t loc;
+};
+
+template <typename T>
+__device__ __forceinline__ void ade_load(const StepArgs<T>& a, const MediumT<T>* media,
+                                         uint32_t w, AdeRec<T>& r) {
+  r.m = (int)((w >> kMediumShift) & 15u);
+  r.loc = w & kLocMask;
+  const MediumT<T>& M = media[r.m];
+  const T* R = a.P + M.poff + (long long)r.loc * (6 * M.npole);
+  if (M.npole == 2) ldv<T, 12>(R, r.v);
+  else if (M.npole == 1) ldv<T, 6>(R, r.v);
 }
 
 // ADE polarisation update and E correction for one dispersive cell
 // (simulation.py:645-669): P^{n+1} = a P^n + b P^{n-1} + c E^n per pole and
-// component, E -= inv * sum_p (P^{n+1} - P^n). P^{n+1} overwrites P^{n-1}.
-template <typename T>
-__device__ __forceinline__ void ade_apply(const StepArgs<T>& a, long long g, const T en[3],
-                                          T e[3]) {
-  const int m = find_medium(a.media, a.n_media, g);
-  const MediumT<T>& M = a.media[m];
-  const long long loc = g - M.base, cnt = M.count;
-  T* P = a.P + M.poff;
-  const int np = M.npole;
-  const int lc = a.lvl, lp = a.lvl ^ 1;
+// component, E -= inv * sum_p (P^{n+1} - P^n), with the Python-float
+// coefficients rounded to the field type as numpy's weak scalars are.
+// P^{n+1} overwrites P^{n-1} (level a.lvl holds P^n). Records with more than
+// two poles are read and written in place.
+// NP-pole update from a loaded record; out[] receives P^{n+1} per
+// [pole][component]. The level of P^n (lc) selects between compile-time
+// record slots, so the record stays in registers.
+template <typename T, int NP>
+__device__ __forceinline__ void ade_np(const MediumT<T>& M, const T* v, int lc, const T en[3],
+                                       T e[3], T out[3 * NP]) {
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     T delta = T(0);
-    for (int p = 0; p < np; ++p) {
-      const long long ic = ((long long)(lc * np + p) * 3 + c) * cnt + loc;
-      const long long ip = ((long long)(lp * np + p) * 3 + c) * cnt + loc;
-      const T pc = P[ic], pp = P[ip];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const T lo = v[p * 3 + c], hi = v[(NP + p) * 3 + c];
+      const T pc = lc ? hi : lo, pp = lc ? lo : hi;
       const T pn = add_rn(add_rn(mul_rn(M.a[p], pc), mul_rn(M.b[p], pp)), mul_rn(M.c[p], en[c]));
-      P[ip] = pn;
+      out[p * 3 + c] = pn;
+      const T inc = sub_rn(pn, pc);
+      delta = p == 0 ? inc : add_rn(delta, inc);
+    }
+    e[c] = sub_rn(e[c], mul_rn(M.inv, delta));
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void ade_update(const StepArgs<T>& a, const MediumT<T>* media,
+                                           const AdeRec<T>& r, const T en[3], T e[3]) {
+  const MediumT<T>& M = media[r.m];
+  const int np = M.npole;
+  T* R = a.P + M.poff + (long long)r.loc * (6 * np);
+  const int lc = a.lvl, lp = a.lvl ^ 1;
+  if (np == 2) {
+    T out[6];
+    ade_np<T, 2>(M, r.v, lc, en, e, out);
+    stv<T, 6>(R + lp * 6, out);  // element offset 0 or 6: 8/16-byte aligned
+    return;
+  }
+  if (np == 1) {
+    T out[3];
+    ade_np<T, 1>(M, r.v, lc, en, e, out);
+    R[lp * 3] = out[0];  // offset 3 is odd: scalar stores
+    R[lp * 3 + 1] = out[1];
+    R[lp * 3 + 2] = out[2];
+    return;
+  }
+  for (int c = 0; c < 3; ++c) {
+    T delta = T(0);
+    for (int p = 0; p < np; ++p) {
+      const T pc = R[(lc * np + p) * 3 + c], pp = R[(lp * np + p) * 3 + c];
+      const T pn = add_rn(add_rn(mul_rn(M.a[p], pc), mul_rn(M.b[p], pp)), mul_rn(M.c[p], en[c]));
+      R[(lp * np + p) * 3 + c] = pn;
       const T inc = sub_rn(pn, pc);
       delta = p == 0 ? inc : add_rn(delta, inc);
     }
@@ -214,30 +300,27 @@ __device__ __forceinline__ void ade_apply(const StepArgs<T>& a, long long g, con
   }
 }
 
-// E-update coefficients of one cell and its compact dispersive index (-1 if
-// the cell is not dispersive).
+// E-update coefficients of one cell and, for a dispersive cell, its ADE
+// word (0 for a plain cell).
 template <typename T, int CE, bool ADE>
-__device__ __forceinline__ void cell_coeffs(const StepArgs<T>& a, long long id, T K[3],
-                                            long long& g) {
-  g = -1;
+__device__ __forceinline__ void cell_coeffs(const StepArgs<T>& a, const MediumT<T>* media,
+                                            long long id, T K[3], uint32_t& w) {
+  w = 0u;
   if (CE == kCeCell1) {
     K[0] = K[1] = K[2] = a.ce[0][id];
+    if (ADE) w = a.adeword[id];
   } else if (CE == kCeCell3) {
     K[0] = a.ce[0][id];
     K[1] = a.ce[1][id];
     K[2] = a.ce[2][id];
   } else {
-    const uint32_t w = a.word[id];
-    if (ADE && (w & kDispersiveBit)) {
-      g = (long long)(w & ~kDispersiveBit);
-      K[0] = K[1] = K[2] = a.media[find_medium(a.media, a.n_media, g)].ce;
+    const uint32_t t = a.word[id];
+    if (ADE && (t & kDispersiveBit)) {
+      w = t;
+      K[0] = K[1] = K[2] = media[(t >> kMediumShift) & 15u].ce;
     } else {
-      K[0] = K[1] = K[2] = a.table[w & ~kDispersiveBit];
+      K[0] = K[1] = K[2] = a.table[t & ~kDispersiveBit];
     }
-  }
-  if (ADE && CE == kCeCell1) {
-    const uint32_t w = a.adeword[id];
-    if (w) g = (long long)w - 1;
   }
 }
 

@@ -22,6 +22,36 @@ __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(
 __device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
 __device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
 
+// Correctly rounded a / d given r = RN(1/d), by Markstein's correction:
+// q0 = RN(a * r), rem = a - q0 * d (exact with one FMA), q = RN(q0 + rem * r).
+// The host enables it for a divisor d only after checking that it reproduces
+// IEEE a / d for every float significand of a; the identity is invariant
+// under scaling a by powers of two while a stays in [2^-100, 2^90) and the
+// residual cannot underflow. qdiv_fast first scales a by 2^64 (exact), so
+// every |a| < 2^26 - zero and subnormals included - lands in that window,
+// and scales the quotient back by 2^-64, which is exact while the quotient
+// is normal: guaranteed for d <= 2^-23 (the host requires d in
+// [2^-30, 2^-23]). copysign keeps the sign of a zero quotient. The caller
+// guarantees |a| < 2^26 (qdiv_ok); qdiv checks it itself.
+constexpr float kQdivLimit = 0x1p26f;
+__device__ __forceinline__ float qdiv_fast(float a, float d, float r) {
+  const float as = __fmul_rn(a, 0x1p64f);
+  const float q0 = __fmul_rn(as, r);
+  const float rem = __fmaf_rn(-q0, d, as);
+  return copysignf(__fmul_rn(__fmaf_rn(rem, r, q0), 0x1p-64f), a);
+}
+__device__ __forceinline__ float qdiv(float a, float d, float r, bool fast) {
+  if (fast && fabsf(a) < kQdivLimit) return qdiv_fast(a, d, r);
+  return __fdiv_rn(a, d);
+}
+__device__ __forceinline__ double qdiv_fast(double a, double d, double) { return __ddiv_rn(a, d); }
+__device__ __forceinline__ double qdiv(double a, double d, double, bool) { return __ddiv_rn(a, d); }
+// Whether every numerator of a cell may take qdiv_fast.
+__device__ __forceinline__ bool qdiv_ok(float m) { return m < kQdivLimit; }
+__device__ __forceinline__ bool qdiv_ok(double) { return false; }
+__device__ __forceinline__ float absmax(float a, float b) { return fmaxf(fabsf(a), fabsf(b)); }
+__device__ __forceinline__ double absmax(double a, double b) { return fmax(fabs(a), fabs(b)); }
+
 // Round a double to the field type (round to nearest even).
 __device__ __forceinline__ float to_real(double v, float) { return __double2float_rn(v); }
 __device__ __forceinline__ double to_real(double v, double) { return v; }
@@ -38,23 +68,29 @@ constexpr int kMaxPoles = 8;
 constexpr int kMaxMedia = 16;
 constexpr uint32_t kDispersiveBit = 0x80000000u;
 
-// One dispersive medium as the E kernel sees it (simulation.py:572-636):
-// its cells occupy compact indices [base, base + count); its polarisation
-// state lives at P + poff as [level 0/1][pole][component][count].
+// One dispersive medium as the E kernel sees it (simulation.py:572-636).
+// Its polarisation state is one record per cell, at P + poff + loc * 6 * npole,
+// laid out [level 0/1][pole][component]: a cell's state is contiguous, so a
+// warp reads it with a few vector loads. A dispersive cell's word is
+// kDispersiveBit | medium << kMediumShift | loc.
 template <typename T>
 struct MediumT {
-  long long base, count, poff;
+  long long poff, count;
   int npole;
   T inv;   // 1 / (eps0 * eps_inf), rounded to T as the reference's weak scalar
   T ce;    // dt / (eps_inf * eps0) in table mode
   T a[kMaxPoles], b[kMaxPoles], c[kMaxPoles];
 };
+constexpr int kMediumShift = 27;
+constexpr uint32_t kLocMask = (1u << kMediumShift) - 1u;
 
 // Arguments of one H + E step (split or fused kernels).
 template <typename T>
 struct StepArgs {
   int nx, ny, nz;
   T dx, dy, dz;  // derivative divisors (1 on a collapsed axis)
+  T rdx, rdy, rdz;      // RN(1/d) per axis
+  bool fdx, fdy, fdz;   // reciprocal division verified exact for that axis
   T ch;          // dt / mu0 rounded to T; the H coefficient is -ch
   const T* Ein[3];
   const T* Hin[3];
@@ -73,6 +109,9 @@ struct StepArgs {
   const int* mape[3];
   const int* maph[3];
   int npe[3], nph[3];
+  // Bulk boxes: cells [b0, b1) per axis where the H (hb) or E (eb) update has
+  // both difference terms and no CPML state; they take the straight-line path.
+  int hb0[3], hb1[3], eb0[3], eb1[3];
   // psi: E terms Ex_y, Ex_z, Ey_z, Ey_x, Ez_x, Ez_y; H terms Hx_y, Hx_z,
   // Hy_z, Hy_x, Hz_x, Hz_y (rustbackend.py:200-207 order)
   T* psiE[6];

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -88,7 +89,7 @@ struct pf_engine {
   std::vector<double> h_table;
   std::vector<char> h_cpml[3][4];  // b_e, c_e, b_h, c_h
   int n_media = 0;
-  std::vector<long long> m_base, m_count;
+  std::vector<long long> m_count;
   std::vector<int> m_npole;
   std::vector<double> m_coef, m_inv, m_ce;
   std::vector<uint32_t> h_adeword;
@@ -109,6 +110,7 @@ struct pf_engine {
   int* map_e[3] = {};
   int* map_h[3] = {};
   int npe[3] = {}, nph[3] = {};
+  int hb0[3] = {}, hb1[3] = {}, eb0[3] = {}, eb1[3] = {};
   void* psiE[6] = {};
   void* psiH[2][6] = {};
   void* P = nullptr;
@@ -116,6 +118,8 @@ struct pf_engine {
   double* wave = nullptr;
   int* flag = nullptr;
   bool fused = false;
+  double rdl[3] = {1, 1, 1};     // RN(1/d) in the real type, per axis
+  bool fdiv[3] = {false, false, false};  // reciprocal division verified
   int fused_ty = 8;      // fused tile height (8 or 16), env PFB200_FUSED_TY
   int fused_chunks = 0;  // x chunks per column (0 = auto), env PFB200_XCHUNKS
 
@@ -170,6 +174,28 @@ int upload(pf_engine* e, void** p, const void* src, size_t bytes) {
   if (rc) return rc;
   if (bytes) PF_CUDA(e, cudaMemcpyAsync(*p, src, bytes, cudaMemcpyHostToDevice, e->stream));
   return PF_OK;
+}
+
+// Whether qdiv's reciprocal division (q0 = a*r, rem = fma(-q0, d, a),
+// q = fma(rem, r, q0), r = RN(1/d)) equals IEEE a / d for every float
+// significand a in [1, 2). Sign and binade of a do not change the outcome
+// while nothing over- or underflows; the device's 2^64 prescaling and the
+// range check on d below keep every input of the fast path in that regime.
+// About 8.4M fmaf evaluations (~50 ms).
+bool recip_division_exact(float d) {
+  if (!(d >= 0x1p-30f && d <= 0x1p-23f)) return false;
+  const float r = 1.0f / d;
+  for (uint32_t m = 0; m < (1u << 23); ++m) {
+    const uint32_t bits = 0x3f800000u | m;
+    float a;
+    memcpy(&a, &bits, 4);
+    volatile float q0 = a * r;
+    const float rem = std::fmaf(-q0, d, a);
+    const float q = std::fmaf(rem, r, q0);
+    volatile float ref = a / d;
+    if (q != ref) return false;
+  }
+  return true;
 }
 
 // Bracket one launch of `kind` (0 step, 1 sources, 2 sampling, 3 flush).
@@ -246,6 +272,24 @@ int finalize_typed(pf_engine* e) {
     }
     e->npe[ax] = ce_n;
     e->nph[ax] = ch_n;
+    // Longest run of cells with no psi and both neighbours present: H needs
+    // t <= na-2 (forward difference), E needs t >= 1 (backward difference).
+    auto longest = [&](const std::vector<int>& map, int lo, int hi, int& b0, int& b1) {
+      b0 = b1 = 0;
+      int s0 = -1;
+      for (int t = lo; t <= hi; ++t) {
+        const bool ok = t < hi && map[t] < 0;
+        if (ok && s0 < 0) s0 = t;
+        if (!ok && s0 >= 0) {
+          if (t - s0 > b1 - b0) { b0 = s0; b1 = t; }
+          s0 = -1;
+        }
+      }
+    };
+    if (na > 1) {
+      longest(mh, 0, na - 1, e->hb0[ax], e->hb1[ax]);
+      longest(me, 1, na, e->eb0[ax], e->eb1[ax]);
+    }
     if ((rc = upload(e, (void**)&e->map_e[ax], me.data(), na * 4))) return rc;
     if ((rc = upload(e, (void**)&e->map_h[ax], mh.data(), na * 4))) return rc;
   }
@@ -262,7 +306,8 @@ int finalize_typed(pf_engine* e) {
     for (int lvl = 0; lvl < 2; ++lvl)
       if ((rc = dalloc(e, &e->psiH[lvl][q], eH[q] * S))) return rc;
   }
-  // ADE
+  // ADE: per-medium cell records [level][pole][component], each medium's
+  // block aligned to 4 elements so records load with vector loads
   if (e->n_media > 0) {
     std::vector<MediumT<T>> md(e->n_media);
     long long off = 0;
@@ -270,18 +315,18 @@ int finalize_typed(pf_engine* e) {
     for (int m = 0; m < e->n_media; ++m) {
       MediumT<T>& M = md[m];
       memset(&M, 0, sizeof M);
-      M.base = e->m_base[m];
-      M.count = e->m_count[m];
+      off = (off + 3) & ~3LL;
       M.poff = off;
+      M.count = e->m_count[m];
       M.npole = e->m_npole[m];
       M.inv = (T)e->m_inv[m];
-      M.ce = (T)e->m_ce[m];
+      M.ce = e->m_ce.empty() ? T(0) : (T)e->m_ce[m];
       for (int p = 0; p < M.npole; ++p) {
         M.a[p] = (T)e->m_coef[ci++];
         M.b[p] = (T)e->m_coef[ci++];
         M.c[p] = (T)e->m_coef[ci++];
       }
-      off += 2LL * M.npole * 3 * M.count;
+      off += 6LL * M.npole * M.count;
     }
     if ((rc = dalloc(e, &e->P, off * S))) return rc;
     if ((rc = upload(e, &e->media, md.data(), md.size() * sizeof(MediumT<T>)))) return rc;
@@ -334,7 +379,19 @@ StepArgs<T> step_args(pf_engine* e) {
   a.dx = (T)e->dl[0];
   a.dy = (T)e->dl[1];
   a.dz = (T)e->dl[2];
+  a.rdx = (T)e->rdl[0];
+  a.rdy = (T)e->rdl[1];
+  a.rdz = (T)e->rdl[2];
+  a.fdx = e->fdiv[0];
+  a.fdy = e->fdiv[1];
+  a.fdz = e->fdiv[2];
   a.ch = (T)e->ch;
+  for (int ax = 0; ax < 3; ++ax) {
+    a.hb0[ax] = e->hb0[ax];
+    a.hb1[ax] = e->hb1[ax];
+    a.eb0[ax] = e->eb0[ax];
+    a.eb1[ax] = e->eb1[ax];
+  }
   const int c0 = e->cur, c1 = e->cur ^ 1;
   for (int c = 0; c < 3; ++c) {
     a.Ein[c] = (const T*)e->E[c0][c];
@@ -596,23 +653,22 @@ int pf_set_cpml(pf_engine* e, int axis, const void* b_e, const void* c_e, const 
   return PF_OK;
 }
 
-int pf_set_ade(pf_engine* e, int n_media, const int64_t* base, const int64_t* count,
-               const int32_t* npole, const double* coef, const double* inv_eps, const double* ce_m,
+int pf_set_ade(pf_engine* e, int n_media, const int64_t* count, const int32_t* npole,
+               const double* coef, const double* inv_eps, const double* ce_m,
                const uint32_t* cell_word) {
   if (!e) return PF_ERR_INVALID;
   if (e->finalized) return fail(e, PF_ERR_STATE, "pf_set_ade after pf_finalize");
   if (n_media < 0 || n_media > kMaxMedia)
     return fail(e, PF_ERR_UNSUPPORTED, "at most %d dispersive media, got %d", kMaxMedia, n_media);
   e->n_media = n_media;
-  e->m_base.assign(base, base + n_media);
   e->m_count.assign(count, count + n_media);
   e->m_npole.assign(npole, npole + n_media);
   long long ncoef = 0;
   for (int m = 0; m < n_media; ++m) {
     if (npole[m] < 0 || npole[m] > kMaxPoles)
       return fail(e, PF_ERR_UNSUPPORTED, "at most %d poles per medium, got %d", kMaxPoles, npole[m]);
-    if (m > 0 && base[m] != base[m - 1] + count[m - 1])
-      return fail(e, PF_ERR_INVALID, "media compact ranges must be consecutive");
+    if (count[m] < 0 || count[m] > (long long)kLocMask + 1)
+      return fail(e, PF_ERR_UNSUPPORTED, "at most 2^%d cells per dispersive medium", kMediumShift);
     ncoef += 3LL * npole[m];
   }
   e->m_coef.assign(coef, coef + ncoef);
@@ -620,7 +676,15 @@ int pf_set_ade(pf_engine* e, int n_media, const int64_t* base, const int64_t* co
   e->m_ce.clear();
   if (ce_m) e->m_ce.assign(ce_m, ce_m + n_media);
   e->h_adeword.clear();
-  if (cell_word) e->h_adeword.assign(cell_word, cell_word + e->ncell);
+  if (cell_word) {
+    for (long long q = 0; q < e->ncell; ++q) {
+      const uint32_t w = cell_word[q];
+      if (w && (!(w & kDispersiveBit) || (int)((w >> kMediumShift) & 15u) >= n_media ||
+                (long long)(w & kLocMask) >= count[(w >> kMediumShift) & 15u]))
+        return fail(e, PF_ERR_INVALID, "bad dispersive word 0x%08x at cell %lld", w, q);
+    }
+    e->h_adeword.assign(cell_word, cell_word + e->ncell);
+  }
   return PF_OK;
 }
 
@@ -728,20 +792,47 @@ int pf_finalize(pf_engine* e) {
     return fail(e, PF_ERR_UNSUPPORTED, "dispersive media with a three-component coefficient");
   if (e->n_media > 0 && e->ce_mode == PF_CE_CELL1 && e->h_adeword.size() != (size_t)e->ncell)
     return fail(e, PF_ERR_INVALID, "PF_CE_CELL1 with dispersive media needs cell_word");
+  if (e->ce_mode == PF_CE_TABLE)
+    for (long long q = 0; q < e->ncell; ++q) {
+      const uint32_t w = e->h_word[q];
+      if (!(w & kDispersiveBit)) continue;
+      const uint32_t m = (w >> kMediumShift) & 15u;
+      if ((int)m >= e->n_media || (long long)(w & kLocMask) >= e->m_count[m])
+        return fail(e, PF_ERR_INVALID, "bad dispersive word 0x%08x at cell %lld", w, q);
+    }
   const bool has_h_src = !e->src[1].cell.empty();
   const bool fusable = fused_supported(e->nx, e->ny, e->nz) && !has_h_src;
   if (e->kernel == PF_KERNEL_FUSED && !fusable)
     return fail(e, PF_ERR_UNSUPPORTED, "the fused kernel needs a 3D grid without H-family sources");
-  e->fused = (e->kernel == PF_KERNEL_FUSED) || (e->kernel == PF_KERNEL_AUTO && fusable);
+  // AUTO takes the split passes: on B200 they currently outrun the fused
+  // kernel (measured: config-3 384^3 2.05 vs 2.54 ms/step), whose plane loop
+  // is latency-bound. PF_KERNEL_FUSED selects it explicitly.
+  e->fused = e->kernel == PF_KERNEL_FUSED;
+  (void)fusable;
   if (e->fused) {
     if (const char* v = getenv("PFB200_FUSED_TY")) e->fused_ty = atoi(v) == 16 ? 16 : 8;
     const long long tiles = (long long)((e->nz + 31) / 32) * ((e->ny + e->fused_ty - 1) / e->fused_ty);
     // about one resident wave of blocks (148 SMs x 1024 threads), at least
     // 8 planes per chunk
     int nch = (int)std::max<long long>(1, (148LL * 1024 / (32 * e->fused_ty) + tiles / 2) / tiles);
+    nch = std::max(nch, (e->nx + 11) / 12);  // short chunks hide the plane-loop latency
     nch = std::min(nch, std::max(1, e->nx / 8));
     if (const char* v = getenv("PFB200_XCHUNKS")) nch = std::max(1, atoi(v));
     e->fused_chunks = nch;
+  }
+  if (e->rb == 4) {
+    const int dims[3] = {e->nx, e->ny, e->nz};
+    for (int ax = 0; ax < 3; ++ax) {
+      const float d = (float)e->dl[ax];
+      e->rdl[ax] = (double)(1.0f / d);
+      bool same = false;
+      for (int q = 0; q < ax; ++q)
+        if (dims[q] > 1 && (float)e->dl[q] == d) {
+          e->fdiv[ax] = e->fdiv[q];
+          same = true;
+        }
+      if (!same && dims[ax] > 1 && !getenv("PFB200_IEEE_DIV")) e->fdiv[ax] = recip_division_exact(d);
+    }
   }
   int rc = e->rb == 4 ? finalize_typed<float>(e) : finalize_typed<double>(e);
   if (rc) return rc;
@@ -851,6 +942,17 @@ int pf_read_profile(pf_engine* e, int64_t launches[4], double ms[4], int reset) 
       e->prof_ms[k] = 0.0;
     }
   }
+  return PF_OK;
+}
+
+int pf_info(const pf_engine* e, char* buf, int len) {
+  if (!e || !buf || len < 1) return PF_ERR_INVALID;
+  snprintf(buf, (size_t)len,
+           "kernel=%s fused_ty=%d x_chunks=%d qdiv=%d%d%d ce_mode=%d media=%d real_bytes=%d "
+           "shape=%dx%dx%d dft=%zu flux=%zu",
+           e->fused ? "fused" : "split", e->fused_ty, e->fused_chunks, (int)e->fdiv[0],
+           (int)e->fdiv[1], (int)e->fdiv[2], e->ce_mode, e->n_media, e->rb, e->nx, e->ny, e->nz,
+           e->dfts.size(), e->fluxes.size());
   return PF_OK;
 }
 

@@ -10,6 +10,10 @@
 //   psiA = bA*psiA + cA*dA ; F += (+K)*psiA   (only where cA != 0)
 //   psiB = bB*psiB + cB*dB ; F += (-K)*psiB   (only where cB != 0)
 // with d = (a_hi - a_lo) / dl and K = ce (E) or -ch (H).
+//
+// A block whose cells all lie in the bulk box (both difference terms, no
+// CPML state) takes a straight-line path: the same operations with no
+// extent checks, psi lookups or coefficient loads.
 #pragma once
 
 #include "cell_update.cuh"
@@ -22,17 +26,63 @@ __device__ __forceinline__ T ld_if(const T* f, long long id, long long off, bool
   return cond ? f[id + off] : T(0);
 }
 
+// Three curl updates sharing one magnitude check of their six numerators:
+// out[c] = f[c] + K[c] * (n[2c]/d[2c] - n[2c+1]/d[2c+1]), the divisors in
+// axis order ax[0..5]. The fast exact division applies when every numerator
+// is within its range, otherwise each division is IEEE.
+template <typename T>
+__device__ __forceinline__ void bulk3(const StepArgs<T>& a, const T f[3], const T K[3],
+                                      const T n[6], const int ax[6], T out[3]) {
+  const T dl[3] = {a.dx, a.dy, a.dz};
+  const T rl[3] = {a.rdx, a.rdy, a.rdz};
+  const bool fl[3] = {a.fdx, a.fdy, a.fdz};
+  const T m = absmax(absmax(n[0], n[1]), absmax(absmax(n[2], n[3]), absmax(n[4], n[5])));
+  T q[6];
+  if (a.fdx && a.fdy && a.fdz && qdiv_ok(m)) {
+#pragma unroll
+    for (int t = 0; t < 6; ++t) q[t] = qdiv_fast(n[t], dl[ax[t]], rl[ax[t]]);
+  } else {
+#pragma unroll
+    for (int t = 0; t < 6; ++t) q[t] = qdiv(n[t], dl[ax[t]], rl[ax[t]], fl[ax[t]]);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) out[c] = bulk(f[c], K[c], q[2 * c], q[2 * c + 1]);
+}
+
+__device__ __forceinline__ bool in_box(int i, int j0, int j1, int k0, int k1, const int* b0,
+                                       const int* b1) {
+  return i >= b0[0] && i < b1[0] && j0 >= b0[1] && j1 <= b1[1] && k0 >= b0[2] && k1 <= b1[2];
+}
+
 // H pass: H^{n+1/2} = H^{n-1/2} - ch (curl E^n + psi).
 template <typename T>
 __global__ void __launch_bounds__(256) k_h_split(const __grid_constant__ StepArgs<T> a) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
+  const bool box = in_box(i, blockIdx.y * blockDim.y, (blockIdx.y + 1) * blockDim.y,
+                          blockIdx.x * blockDim.x, (blockIdx.x + 1) * blockDim.x, a.hb0, a.hb1);
   if (k >= a.nz || j >= a.ny) return;
   const long long sy = a.nz, sx = (long long)a.ny * a.nz;
   const long long id = i * sx + j * sy + k;
-  const bool hx = i + 1 < a.nx, hy = j + 1 < a.ny, hz = k + 1 < a.nz;
   const T ex = a.Ein[0][id], ey = a.Ein[1][id], ez = a.Ein[2][id];
+  if (box) {
+    const T f[3] = {a.Hin[0][id], a.Hin[1][id], a.Hin[2][id]};
+    const T mch = -a.ch;
+    const T K[3] = {mch, mch, mch};
+    // Hx: +dEz/dy - dEy/dz; Hy: +dEx/dz - dEz/dx; Hz: +dEy/dx - dEx/dy
+    const T n[6] = {sub_rn(a.Ein[2][id + sy], ez), sub_rn(a.Ein[1][id + 1], ey),
+                    sub_rn(a.Ein[0][id + 1], ex), sub_rn(a.Ein[2][id + sx], ez),
+                    sub_rn(a.Ein[1][id + sx], ey), sub_rn(a.Ein[0][id + sy], ex)};
+    const int ax[6] = {1, 2, 2, 0, 0, 1};
+    T h[3];
+    bulk3<T>(a, f, K, n, ax, h);
+    a.Hout[0][id] = h[0];
+    a.Hout[1][id] = h[1];
+    a.Hout[2][id] = h[2];
+    return;
+  }
+  const bool hx = i + 1 < a.nx, hy = j + 1 < a.ny, hz = k + 1 < a.nz;
   a.Hout[0][id] = upd_hx<T>(a, i, j, k, a.Hin[0][id], ld_if(a.Ein[2], id, sy, hy), ez,
                             ld_if(a.Ein[1], id, 1, hz), ey, true);
   a.Hout[1][id] = upd_hy<T>(a, i, j, k, a.Hin[1][id], ld_if(a.Ein[0], id, 1, hz), ex,
@@ -47,23 +97,36 @@ __global__ void __launch_bounds__(256) k_e_split(const __grid_constant__ StepArg
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
+  const bool box = in_box(i, blockIdx.y * blockDim.y, (blockIdx.y + 1) * blockDim.y,
+                          blockIdx.x * blockDim.x, (blockIdx.x + 1) * blockDim.x, a.eb0, a.eb1);
   if (k >= a.nz || j >= a.ny) return;
   const long long sy = a.nz, sx = (long long)a.ny * a.nz;
   const long long id = i * sx + j * sy + k;
   T K[3];
-  long long g;
-  cell_coeffs<T, CE, ADE>(a, id, K, g);
+  uint32_t w;
+  cell_coeffs<T, CE, ADE>(a, a.media, id, K, w);
+  AdeRec<T> rec;
+  if (ADE && w) ade_load<T>(a, a.media, w, rec);
   const T hx = a.Hin[0][id], hy = a.Hin[1][id], hz = a.Hin[2][id];
-  const bool lx = i > 0, ly = j > 0, lz = k > 0;
   T en[3] = {a.Ein[0][id], a.Ein[1][id], a.Ein[2][id]};
   T e[3];
-  e[0] = upd_ex<T>(a, i, j, k, en[0], K[0], hz, ld_if(a.Hin[2], id, -sy, ly), hy,
-                   ld_if(a.Hin[1], id, -1, lz));
-  e[1] = upd_ey<T>(a, i, j, k, en[1], K[1], hx, ld_if(a.Hin[0], id, -1, lz), hz,
-                   ld_if(a.Hin[2], id, -sx, lx));
-  e[2] = upd_ez<T>(a, i, j, k, en[2], K[2], hy, ld_if(a.Hin[1], id, -sx, lx), hx,
-                   ld_if(a.Hin[0], id, -sy, ly));
-  if (ADE && g >= 0) ade_apply<T>(a, g, en, e);
+  if (box) {
+    // Ex: +dHz/dy - dHy/dz; Ey: +dHx/dz - dHz/dx; Ez: +dHy/dx - dHx/dy
+    const T n[6] = {sub_rn(hz, a.Hin[2][id - sy]), sub_rn(hy, a.Hin[1][id - 1]),
+                    sub_rn(hx, a.Hin[0][id - 1]), sub_rn(hz, a.Hin[2][id - sx]),
+                    sub_rn(hy, a.Hin[1][id - sx]), sub_rn(hx, a.Hin[0][id - sy])};
+    const int ax[6] = {1, 2, 2, 0, 0, 1};
+    bulk3<T>(a, en, K, n, ax, e);
+  } else {
+    const bool lx = i > 0, ly = j > 0, lz = k > 0;
+    e[0] = upd_ex<T>(a, i, j, k, en[0], K[0], hz, ld_if(a.Hin[2], id, -sy, ly), hy,
+                     ld_if(a.Hin[1], id, -1, lz));
+    e[1] = upd_ey<T>(a, i, j, k, en[1], K[1], hx, ld_if(a.Hin[0], id, -1, lz), hz,
+                     ld_if(a.Hin[2], id, -sx, lx));
+    e[2] = upd_ez<T>(a, i, j, k, en[2], K[2], hy, ld_if(a.Hin[1], id, -sx, lx), hx,
+                     ld_if(a.Hin[0], id, -sy, ly));
+  }
+  if (ADE && w) ade_update<T>(a, a.media, rec, en, e);
   a.Eout[0][id] = e[0];
   a.Eout[1][id] = e[1];
   a.Eout[2][id] = e[2];

@@ -209,24 +209,26 @@ def build_tables(sim) -> dict:
         t["table"] = (dt / (vals * EPS_0)).astype(edt, copy=False).astype(np.float64)
         t["word"] = word
     if ade is not None:
+        # dispersive word: bit 31 | medium << 27 | rank of the cell among the
+        # medium's cells in C order
+        if any(c > (1 << 27) for c in ade["count"]):
+            raise NotImplementedError("more than 2^27 cells in one dispersive medium")
         flat_word = np.zeros(int(np.prod(grid.shape)), dtype=np.uint32)
         ce_m = []
         for m, med in enumerate(ade["media"]):
-            g0 = int(ade["base"][m])
-            flat_word[ade["cells"][m]] = np.arange(g0, g0 + ade["cells"][m].size, dtype=np.uint32)
+            cells = ade["cells"][m]
+            flat_word[cells] = (np.uint32(0x80000000) | np.uint32(m << 27)
+                                | np.arange(cells.size, dtype=np.uint32))
             # the coefficient a dispersive cell gets from its stamped eps_inf
             ce_m.append(float((dt / (np.array([med.eps_r], dtype=edt) * EPS_0)).astype(edt)[0]))
         ade["ce_m"] = np.array(ce_m, np.float64)
         if t["ce_mode"] == N.PF_CE_TABLE:
             w = t["word"].ravel()
             for m in range(len(ade["media"])):
-                w[ade["cells"][m]] = np.uint32(0x80000000) | flat_word[ade["cells"][m]]
+                w[ade["cells"][m]] = flat_word[ade["cells"][m]]
             ade["cell_word"] = None
         else:
-            cw = np.zeros_like(flat_word)
-            for m in range(len(ade["media"])):
-                cw[ade["cells"][m]] = flat_word[ade["cells"][m]] + 1
-            ade["cell_word"] = cw
+            ade["cell_word"] = flat_word
         del ade["cells"]
     t["ade"] = ade
     t["sources"] = source_tables(sim, n_steps, dt)
@@ -332,8 +334,8 @@ class B200Engine:
         ade = t["ade"]
         if ade is not None:
             cw = ade["cell_word"]
-            self._chk(L.pf_set_ade(h, len(ade["media"]), N.ptr(ade["base"], C.c_int64),
-                                   N.ptr(ade["count"], C.c_int64), N.ptr(ade["npole"], C.c_int32),
+            self._chk(L.pf_set_ade(h, len(ade["media"]), N.ptr(ade["count"], C.c_int64),
+                                   N.ptr(ade["npole"], C.c_int32),
                                    N.ptr(ade["coef"], C.c_double), N.ptr(ade["inv"], C.c_double),
                                    N.ptr(ade["ce_m"], C.c_double),
                                    None if cw is None else N.ptr(cw, C.c_uint32)))
@@ -405,6 +407,13 @@ class B200Engine:
         ms = (C.c_double * 4)()
         self._chk(self._L.pf_read_profile(self.h, n, ms, 1 if reset else 0))
         return list(n), list(ms)
+
+    def info(self) -> dict:
+        """Engine configuration (kernel path, tiling, division mode, ...)."""
+        import ctypes as C
+        buf = C.create_string_buffer(512)
+        self._chk(self._L.pf_info(self.h, buf, 512))
+        return dict(kv.split("=", 1) for kv in buf.value.decode().split())
 
     def device_bytes(self) -> int:
         import ctypes as C
