@@ -37,6 +37,7 @@ extern "C" {
 #define PF_ERR_CUDA (-2)        /* a CUDA runtime call failed           */
 #define PF_ERR_OOM (-3)         /* device allocation failed             */
 #define PF_ERR_NONFINITE (-4)   /* non-finite field found by pf_check   */
+#define PF_ERR_TIMEOUT (-5)     /* a bounded device wait ran out        */
 #define PF_ERR_UNSUPPORTED (-6) /* feature combination not implemented  */
 #define PF_ERR_STATE (-7)       /* engine not finalised / finalised     */
 

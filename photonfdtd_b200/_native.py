@@ -15,6 +15,7 @@ PF_ERR_INVALID = -1
 PF_ERR_CUDA = -2
 PF_ERR_OOM = -3
 PF_ERR_NONFINITE = -4
+PF_ERR_TIMEOUT = -5
 PF_ERR_UNSUPPORTED = -6
 PF_ERR_STATE = -7
 

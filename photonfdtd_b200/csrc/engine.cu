@@ -24,6 +24,7 @@
 #include "kernels_aux.cuh"
 #include "kernels_fused.cuh"
 #include "kernels_split.cuh"
+#include "kernels_tma.cuh"
 
 using namespace pfb;
 
@@ -120,6 +121,9 @@ struct pf_engine {
   bool fused = false;
   double rdl[3] = {1, 1, 1};     // RN(1/d) in the real type, per axis
   bool fdiv[3] = {false, false, false};  // reciprocal division verified
+  bool tma = false;      // fused path stages planes with TMA
+  TmaMaps maps;
+  int* tma_err = nullptr;
   int fused_ty = 8;      // fused tile height (8 or 16), env PFB200_FUSED_TY
   int fused_chunks = 0;  // x chunks per column (0 = auto), env PFB200_XCHUNKS
 
@@ -229,6 +233,62 @@ void collect_profile(pf_engine* e) {
   }
   e->ev_pending.clear();
   e->ev_used = 0;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+// Tiled map over a C-order (nx, ny, nz) array, box (bw along z) x (bh along y)
+// x 1 plane. Zero fill outside the array.
+bool make_map(CUtensorMap* m, void* ptr, CUtensorMapDataType dt, int elem, int nx, int ny, int nz,
+              int bw, int bh) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)nz, (cuuint64_t)ny, (cuuint64_t)nx};
+  const cuuint64_t strides[2] = {(cuuint64_t)nz * elem, (cuuint64_t)ny * nz * elem};
+  const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return enc(m, dt, 3, ptr, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Tensor maps of the TMA fused path (tile height 8); false if any fails.
+template <typename T>
+bool build_maps(pf_engine* e) {
+  const CUtensorMapDataType dt =
+      sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+  const int S = sizeof(T), TY = 8;
+  memset(&e->maps, 0, sizeof e->maps);
+  bool ok = true;
+  for (int l = 0; l < 2; ++l)
+    for (int c = 0; c < 3; ++c) {
+      ok = ok && make_map(&e->maps.e[l][c], e->E[l][c], dt, S, e->nx, e->ny, e->nz, kBoxW, TY + 2);
+      ok = ok && make_map(&e->maps.h[l][c], e->H[l][c], dt, S, e->nx, e->ny, e->nz, kBoxW, TY + 1);
+    }
+  void* wptr = e->ce_mode == PF_CE_TABLE ? (void*)e->word : (void*)e->adeword;
+  if (wptr)
+    ok = ok && make_map(&e->maps.word, wptr, CU_TENSOR_MAP_DATA_TYPE_UINT32, 4, e->nx, e->ny,
+                        e->nz, 32, TY);
+  if (e->ce_mode != PF_CE_TABLE)
+    for (int c = 0; c < 3; ++c)
+      ok = ok && make_map(&e->maps.ce[c], e->ce[c], dt, S, e->nx, e->ny, e->nz, 32, TY);
+  return ok;
 }
 
 template <typename T>
@@ -365,6 +425,11 @@ int finalize_typed(pf_engine* e) {
     if ((rc = dalloc(e, (void**)&f.acc, 8))) return rc;
   }
   if ((rc = dalloc(e, (void**)&e->flag, sizeof(int)))) return rc;
+  if ((rc = dalloc(e, (void**)&e->tma_err, sizeof(int)))) return rc;
+  // TMA staging needs 16-byte row strides (nz * sizeof(T) % 16 == 0)
+  if (e->fused && !getenv("PFB200_NO_TMA") && ((long long)e->nz * S) % 16 == 0 &&
+      !(e->n_media > 0 && e->ce_mode == PF_CE_CELL3))
+    e->tma = build_maps<T>(e);
   PF_CUDA(e, cudaStreamSynchronize(e->stream));
   return PF_OK;
 }
@@ -526,8 +591,12 @@ int advance_typed(pf_engine* e, long long n_sub) {
       int rc;
       {
         LaunchScope ls(e, 0);
-        rc = launch_fused<T>(e->stream, a, e->ce_mode, e->n_media > 0, e->fused_ty,
-                             e->fused_chunks);
+        if (e->tma)
+          rc = launch_tma<T>(e->stream, a, e->maps, e->cur, e->ce_mode, e->n_media > 0,
+                             e->fused_chunks, e->tma_err);
+        else
+          rc = launch_fused<T>(e->stream, a, e->ce_mode, e->n_media > 0, e->fused_ty,
+                               e->fused_chunks);
       }
       if (rc) return fail(e, PF_ERR_UNSUPPORTED, "fused kernel does not cover this case");
       // sources of the fused path are injected after its single pass: an H
@@ -557,6 +626,12 @@ int advance_typed(pf_engine* e, long long n_sub) {
   PF_CUDA(e, cudaGetLastError());
   PF_CUDA(e, cudaStreamSynchronize(e->stream));
   collect_profile(e);
+  if (e->tma) {
+    int h = 0;
+    PF_CUDA(e, cudaMemcpy(&h, e->tma_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h == 2) return fail(e, PF_ERR_CUDA, "TMA staging buffer misaligned; results are invalid");
+    if (h) return fail(e, PF_ERR_TIMEOUT, "a TMA stage wait timed out; results are invalid");
+  }
   return PF_OK;
 }
 
@@ -949,9 +1024,11 @@ int pf_info(const pf_engine* e, char* buf, int len) {
   if (!e || !buf || len < 1) return PF_ERR_INVALID;
   snprintf(buf, (size_t)len,
            "kernel=%s fused_ty=%d x_chunks=%d qdiv=%d%d%d ce_mode=%d media=%d real_bytes=%d "
+           "tma=%d "
            "shape=%dx%dx%d dft=%zu flux=%zu",
            e->fused ? "fused" : "split", e->fused_ty, e->fused_chunks, (int)e->fdiv[0],
-           (int)e->fdiv[1], (int)e->fdiv[2], e->ce_mode, e->n_media, e->rb, e->nx, e->ny, e->nz,
+           (int)e->fdiv[1], (int)e->fdiv[2], e->ce_mode, e->n_media, e->rb, (int)e->tma, e->nx,
+           e->ny, e->nz,
            e->dfts.size(), e->fluxes.size());
   return PF_OK;
 }
