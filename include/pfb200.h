@@ -184,6 +184,31 @@ int pf_device_bytes(const pf_engine *eng, int64_t *bytes);
 /* Release everything. NULL is a no-op. */
 void pf_destroy(pf_engine *eng);
 
+/* Poynting flux of one plane of one time level, allocating no device memory.
+ * No counterpart in the reference: it is this library's flux reduction for
+ * callers that cannot allocate device memory on their call path - a process
+ * whose device memory belongs to another allocator (a framework's caching
+ * pool, a server that reserved its whole budget up front), code that only
+ * borrows field buffers and holds no allocator, or a time loop that must not
+ * pay cudaMalloc's device-wide synchronisation.
+ * fields: six device pointers Ex, Ey, Ez, Hx, Hy, Hz, C-order (nx, ny, nz) in
+ * the real type. Writes, on `stream` (a cudaStream_t, NULL = default stream),
+ * *out = double(T(sum S) * T(dA)) * dt into the caller's device double - the
+ * quantity the engine's flux monitor adds per step. Asynchronous: read *out
+ * after the stream has done.
+ * Scratch: the per-block partial sums live in one fixed device array of
+ * 65,536 doubles (512 KB) per GPU that loads the library, kept until the
+ * process exits; planes of more than 16,777,216 cells are rejected with
+ * PF_ERR_INVALID. The first call on a device resolves that array's address
+ * with the device current, so make the first call before any stream capture.
+ * Every call shares the array and each call writes all partials it reads, so
+ * no state carries between calls; calls that overlap on the GPU (other
+ * streams or threads) race on it. Error text: pf_noalloc_last_error(). */
+int pf_flux_plane_noalloc(int real_bytes, int nx, int ny, int nz,
+                          const void *const fields[6], int axis, int idx,
+                          double dA, double dt, double *out, void *stream);
+const char *pf_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

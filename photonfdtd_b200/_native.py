@@ -63,6 +63,9 @@ SIGNATURES = {
     "pf_read_profile": (C.c_int, [_vp, _pi64, _pdbl, C.c_int]),
     "pf_info": (C.c_int, [_vp, C.c_char_p, C.c_int]),
     "pf_destroy": (None, [_vp]),
+    "pf_flux_plane_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_vp),
+                                        C.c_int, C.c_int, _dbl, _dbl, _vp, _vp]),
+    "pf_noalloc_last_error": (C.c_char_p, []),
 }
 
 
