@@ -16,7 +16,7 @@
 // extent checks, psi lookups or coefficient loads.
 #pragma once
 
-#include "cell_update.cuh"
+#include "cell3d.cuh"
 
 namespace pfb {
 
@@ -83,6 +83,18 @@ __global__ void __launch_bounds__(256) k_h_split(const __grid_constant__ StepArg
     return;
   }
   const bool hx = i + 1 < a.nx, hy = j + 1 < a.ny, hz = k + 1 < a.nz;
+  if (a.nx > 1 && a.ny > 1 && a.nz > 1) {
+    const T hold[3] = {a.Hin[0][id], a.Hin[1][id], a.Hin[2][id]};
+    const T n[6] = {sub_rn(ld_if(a.Ein[2], id, sy, hy), ez), sub_rn(ld_if(a.Ein[1], id, 1, hz), ey),
+                    sub_rn(ld_if(a.Ein[0], id, 1, hz), ex), sub_rn(ld_if(a.Ein[2], id, sx, hx), ez),
+                    sub_rn(ld_if(a.Ein[1], id, sx, hx), ey), sub_rn(ld_if(a.Ein[0], id, sy, hy), ex)};
+    T h[3];
+    h3<T>(a, i, j, k, hold, n, true, h);
+    a.Hout[0][id] = h[0];
+    a.Hout[1][id] = h[1];
+    a.Hout[2][id] = h[2];
+    return;
+  }
   a.Hout[0][id] = upd_hx<T>(a, i, j, k, a.Hin[0][id], ld_if(a.Ein[2], id, sy, hy), ez,
                             ld_if(a.Ein[1], id, 1, hz), ey, true);
   a.Hout[1][id] = upd_hy<T>(a, i, j, k, a.Hin[1][id], ld_if(a.Ein[0], id, 1, hz), ex,
@@ -117,6 +129,12 @@ __global__ void __launch_bounds__(256) k_e_split(const __grid_constant__ StepArg
                     sub_rn(hy, a.Hin[1][id - sx]), sub_rn(hx, a.Hin[0][id - sy])};
     const int ax[6] = {1, 2, 2, 0, 0, 1};
     bulk3<T>(a, en, K, n, ax, e);
+  } else if (a.nx > 1 && a.ny > 1 && a.nz > 1) {
+    const bool lx = i > 0, ly = j > 0, lz = k > 0;
+    const T n[6] = {sub_rn(hz, ld_if(a.Hin[2], id, -sy, ly)), sub_rn(hy, ld_if(a.Hin[1], id, -1, lz)),
+                    sub_rn(hx, ld_if(a.Hin[0], id, -1, lz)), sub_rn(hz, ld_if(a.Hin[2], id, -sx, lx)),
+                    sub_rn(hy, ld_if(a.Hin[1], id, -sx, lx)), sub_rn(hx, ld_if(a.Hin[0], id, -sy, ly))};
+    e3<T>(a, i, j, k, en, K, n, e);
   } else {
     const bool lx = i > 0, ly = j > 0, lz = k > 0;
     e[0] = upd_ex<T>(a, i, j, k, en[0], K[0], hz, ld_if(a.Hin[2], id, -sy, ly), hy,

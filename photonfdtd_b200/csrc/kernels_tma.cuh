@@ -19,7 +19,7 @@
 
 #include <cuda.h>
 
-#include "cell_update.cuh"
+#include "cell3d.cuh"
 
 namespace pfb {
 
@@ -199,6 +199,7 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY))
     const Stage& S0 = st[q0 % NS];
     const Stage& S1 = st[q1 % NS];
     const int id = i * sx + colid;
+
     const bool fast = yz_bulk && i >= xb0 && i < xb1;
 
     // coefficients and ADE state of plane i
@@ -259,26 +260,36 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY))
       }
     } else {
       if (own) {
-        hx = upd_hx<T>(a, i, j, k, H0[0][jj][kz], E0[2][jj + 1][kz], E0[2][jj][kz], E0[1][jj][kz + 1],
-                       E0[1][jj][kz], true);
-        hy = upd_hy<T>(a, i, j, k, H0[1][jj][kz], E0[0][jj][kz + 1], E0[0][jj][kz], E1[2][jj][kz],
-                       E0[2][jj][kz], true);
-        hz = upd_hz<T>(a, i, j, k, H0[2][jj][kz], E1[1][jj][kz], E0[1][jj][kz], E0[0][jj + 1][kz],
-                       E0[0][jj][kz], true);
+        const T hold[3] = {H0[0][jj][kz], H0[1][jj][kz], H0[2][jj][kz]};
+        const T n[6] = {sub_rn(E0[2][jj + 1][kz], E0[2][jj][kz]), sub_rn(E0[1][jj][kz + 1], E0[1][jj][kz]),
+                        sub_rn(E0[0][jj][kz + 1], E0[0][jj][kz]), sub_rn(E1[2][jj][kz], E0[2][jj][kz]),
+                        sub_rn(E1[1][jj][kz], E0[1][jj][kz]), sub_rn(E0[0][jj + 1][kz], E0[0][jj][kz])};
+        T h[3];
+        h3<T>(a, i, j, k, hold, n, true, h);
+        hx = h[0];
+        hy = h[1];
+        hz = h[2];
       }
-      if (row_h) {
-        const int jr = j0 - 1;
-        sh[0][0][tz + 1] = upd_hx<T>(a, i, jr, k, H0[0][0][kz], E0[2][1][kz], E0[2][0][kz],
-                                     E0[1][0][kz + 1], E0[1][0][kz], false);
-        sh[2][0][tz + 1] = upd_hz<T>(a, i, jr, k, H0[2][0][kz], E1[1][0][kz], E0[1][0][kz],
-                                     E0[0][1][kz], E0[0][0][kz], false);
+      if (row_h) {  // Hx and Hz at y = j0-1 (Hy computed and dropped)
+        const T hold[3] = {H0[0][0][kz], H0[1][0][kz], H0[2][0][kz]};
+        const T n[6] = {sub_rn(E0[2][1][kz], E0[2][0][kz]), sub_rn(E0[1][0][kz + 1], E0[1][0][kz]),
+                        sub_rn(E0[0][0][kz + 1], E0[0][0][kz]), sub_rn(E1[2][0][kz], E0[2][0][kz]),
+                        sub_rn(E1[1][0][kz], E0[1][0][kz]), sub_rn(E0[0][1][kz], E0[0][0][kz])};
+        T h[3];
+        h3<T>(a, i, j0 - 1, k, hold, n, false, h);
+        sh[0][0][tz + 1] = h[0];
+        sh[2][0][tz + 1] = h[2];
       }
-      if (col_h) {
-        const int jr = j0 + tcol, kc = k0 - 1, r = tcol + 1, c3 = kBoxZ0 - 1;
-        sh[0][r][0] = upd_hx<T>(a, i, jr, kc, H0[0][r][c3], E0[2][r + 1][c3], E0[2][r][c3],
-                                E0[1][r][c3 + 1], E0[1][r][c3], false);
-        sh[1][r][0] = upd_hy<T>(a, i, jr, kc, H0[1][r][c3], E0[0][r][c3 + 1], E0[0][r][c3],
-                                E1[2][r][c3], E0[2][r][c3], false);
+      if (col_h) {  // Hx and Hy at z = k0-1 (Hz computed and dropped)
+        const int r = tcol + 1, c3 = kBoxZ0 - 1;
+        const T hold[3] = {H0[0][r][c3], H0[1][r][c3], H0[2][r][c3]};
+        const T n[6] = {sub_rn(E0[2][r + 1][c3], E0[2][r][c3]), sub_rn(E0[1][r][c3 + 1], E0[1][r][c3]),
+                        sub_rn(E0[0][r][c3 + 1], E0[0][r][c3]), sub_rn(E1[2][r][c3], E0[2][r][c3]),
+                        sub_rn(E1[1][r][c3], E0[1][r][c3]), sub_rn(E0[0][r + 1][c3], E0[0][r][c3])};
+        T h[3];
+        h3<T>(a, i, j0 + tcol, k0 - 1, hold, n, false, h);
+        sh[0][r][0] = h[0];
+        sh[1][r][0] = h[1];
       }
     }
     if (own) {
@@ -310,9 +321,10 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY))
           e[2] = bulk(en[2], K[2], qdiv(n4, a.dx, a.rdx, a.fdx), qdiv(n5, a.dy, a.rdy, a.fdy));
         }
       } else {
-        e[0] = upd_ex<T>(a, i, j, k, en[0], K[0], hz, sh[2][jj - 1][kk], hy, sh[1][jj][kk - 1]);
-        e[1] = upd_ey<T>(a, i, j, k, en[1], K[1], hx, sh[0][jj][kk - 1], hz, hz_prev);
-        e[2] = upd_ez<T>(a, i, j, k, en[2], K[2], hy, hy_prev, hx, sh[0][jj - 1][kk]);
+        const T n[6] = {sub_rn(hz, sh[2][jj - 1][kk]), sub_rn(hy, sh[1][jj][kk - 1]),
+                        sub_rn(hx, sh[0][jj][kk - 1]), sub_rn(hz, hz_prev),
+                        sub_rn(hy, hy_prev), sub_rn(hx, sh[0][jj - 1][kk])};
+        e3<T>(a, i, j, k, en, K, n, e);
       }
       if (ADE && w) ade_update<T>(a, media, rec, en, e);
       a.Eout[0][id] = e[0];
