@@ -209,6 +209,87 @@ int pf_flux_plane_noalloc(int real_bytes, int nx, int ny, int nz,
                           double dA, double dt, double *out, void *stream);
 const char *pf_noalloc_last_error(void);
 
+/* ------------------------------------------------------------------------
+ * Batched 2D TE engine with a discrete adjoint (pf_batch).
+ *
+ * Many 2D instances (xy plane, nz = 1) of uneven size, stepped together on
+ * one stream: Hz, Ex, Ey with CPML on x and y, per-cell E coefficient
+ * K = dt/(eps*eps0), soft sources and one output-line DFT of Ey per instance.
+ * It replaces the reference's per-simulation gradient path for this problem:
+ * jax_value_and_grad_eps / value_and_grad_eps (src/photonfdtd/
+ * jaxbackend.py:666-722, remat checkpointing :511-570) and its reversible
+ * variants (src/photonfdtd/reversible_pml.py:100-209), whose stepping is
+ * simulation.py:1252-1309 restricted to TE with nz = 1. The forward fields
+ * and DFT match the reference's NumPy run of each instance to the bit.
+ *
+ * Sequence: pfb_create, pfb_set_instance (each k), pfb_set_sources,
+ * pfb_set_dft, pfb_finalize; then per design iteration pfb_set_design_ce,
+ * pfb_forward, pfb_read_dft, pfb_adjoint(cotangent), pfb_read_grad.
+ * Packed layouts: line cells in instance order, ny_k per instance (the x
+ * index line_i, every y); design cells in instance order, dn_k * dn_k each,
+ * C order (i, j) inside the window.
+ * ---------------------------------------------------------------------- */
+typedef struct pf_batch pf_batch;
+
+/* n_inst instances sharing dx, dy, ch = dt/mu0 (real type), dt and n_steps. */
+int pfb_create(int n_inst, int real_bytes, double dx, double dy, double ch, double dt,
+               int64_t n_steps, pf_batch **out);
+
+/* Instance k: grid nx x ny, ce (nx*ny reals, C order), CPML coefficient
+ * arrays coef = {b_e_x, c_e_x, b_h_x, c_h_x (nx each), b_e_y, c_e_y, b_h_y,
+ * c_h_y (ny each)} (simulation.py:794-808), the design window
+ * [di0, di0+dn) x [dj0, dj0+dn) whose coefficient gradient is returned, and
+ * the x index of the output line. */
+int pfb_set_instance(pf_batch *b, int k, int nx, int ny, const void *ce,
+                     const void *const coef[8], int di0, int dj0, int dn, int line_i);
+
+/* Soft sources (simulation.py:1367-1390): source q adds amp[q] *
+ * wave[wave_row[q]][n] to component comp[q] (0 Ex, 1 Ey, 2 Hz) of instance
+ * inst[q] at (i[q], j[q]) in step n; wave is (n_wave, n_steps) doubles,
+ * already evaluated at the family's times. Sources on one cell are added in
+ * list order. */
+int pfb_set_sources(pf_batch *b, int n_src, const int32_t *inst, const int32_t *comp,
+                    const int32_t *i, const int32_t *j, const int32_t *wave_row,
+                    const double *amp, int n_wave, const double *wave);
+
+/* DFT phases: phase[n][f] = exp(i w_f (n+1) dt) as (re, im) doubles,
+ * n_steps x n_freq (simulation.py:1116-1133). */
+int pfb_set_dft(pf_batch *b, int n_freq, const double *phase);
+
+/* Lays out the pooled arrays and uploads everything. checkpoint_every = K:
+ * the state is stored every K steps (ceil(n_steps/K) - 1 states), and the
+ * adjoint replays K steps at a time; K >= n_steps stores no state and needs
+ * no replay. tile_rows: x rows per 32-wide tile (4, 8 or 16). */
+int pfb_finalize(pf_batch *b, int checkpoint_every, int tile_rows);
+
+/* Replaces the design-window coefficients of every instance from a packed
+ * host array (n_design reals). */
+int pfb_set_design_ce(pf_batch *b, const void *ce_design);
+
+/* Runs all n_steps from zero fields; the DFT accumulators hold the result. */
+int pfb_forward(pf_batch *b);
+
+/* Reverse pass for the loss whose DFT cotangent is `cotangent`: packed line
+ * cells x n_freq complex (re, im) doubles, G = dL/dRe F + i dL/dIm F.
+ * Afterwards pfb_read_grad gives dL/dK of every design cell. May be called
+ * again after the same forward with another cotangent. Leaves the forward
+ * fields overwritten (pfb_read_field then shows a replayed state). */
+int pfb_adjoint(pf_batch *b, const double *cotangent);
+
+/* Packed DFT accumulators (line cells x n_freq complex doubles). */
+int pfb_read_dft(pf_batch *b, double *dst);
+/* Packed dL/dK of the design cells (doubles). */
+int pfb_read_grad(pf_batch *b, double *dst);
+/* Component comp (0 Ex, 1 Ey, 2 Hz) of instance k, nx*ny reals. */
+int pfb_read_field(pf_batch *b, int k, int comp, void *dst);
+/* out[0..n_out): cells, line cells, design cells, tiles, K, segments,
+ * reals per stored state, kernel launches issued so far. */
+int pfb_info(const pf_batch *b, int64_t *out, int n_out);
+/* The batch's cudaStream_t. */
+void *pfb_stream(pf_batch *b);
+const char *pfb_last_error(const pf_batch *b);
+void pfb_destroy(pf_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

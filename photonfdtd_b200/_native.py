@@ -66,6 +66,24 @@ SIGNATURES = {
     "pf_flux_plane_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_vp),
                                         C.c_int, C.c_int, _dbl, _dbl, _vp, _vp]),
     "pf_noalloc_last_error": (C.c_char_p, []),
+    # batched 2D TE engine with adjoint
+    "pfb_create": (C.c_int, [C.c_int, C.c_int, _dbl, _dbl, _dbl, _dbl, _i64, C.POINTER(_vp)]),
+    "pfb_set_instance": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, C.POINTER(_vp), C.c_int,
+                                   C.c_int, C.c_int, C.c_int]),
+    "pfb_set_sources": (C.c_int, [_vp, C.c_int, _pi32, _pi32, _pi32, _pi32, _pi32, _pdbl,
+                                  C.c_int, _pdbl]),
+    "pfb_set_dft": (C.c_int, [_vp, C.c_int, _pdbl]),
+    "pfb_finalize": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "pfb_set_design_ce": (C.c_int, [_vp, _vp]),
+    "pfb_forward": (C.c_int, [_vp]),
+    "pfb_adjoint": (C.c_int, [_vp, _pdbl]),
+    "pfb_read_dft": (C.c_int, [_vp, _pdbl]),
+    "pfb_read_grad": (C.c_int, [_vp, _pdbl]),
+    "pfb_read_field": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
+    "pfb_info": (C.c_int, [_vp, _pi64, C.c_int]),
+    "pfb_stream": (_vp, [_vp]),
+    "pfb_last_error": (C.c_char_p, [_vp]),
+    "pfb_destroy": (None, [_vp]),
 }
 
 
@@ -97,10 +115,12 @@ class NativeError(RuntimeError):
         self.code = code
 
 
-def check(rc: int, handle=None) -> None:
+def check(rc: int, handle=None, batch: bool = False) -> None:
+    """Raise for a non-OK return code; ``batch`` selects the pf_batch error text."""
     if rc == PF_OK:
         return
-    msg = lib().pf_last_error(handle).decode(errors="replace")
+    L = lib()
+    msg = (L.pfb_last_error(handle) if batch else L.pf_last_error(handle)).decode(errors="replace")
     if rc == PF_ERR_UNSUPPORTED:
         raise NotImplementedError(msg)
     if rc == PF_ERR_INVALID:

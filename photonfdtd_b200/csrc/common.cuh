@@ -126,4 +126,8 @@ struct StepArgs {
 
 enum CeMode { kCeCell1 = 0, kCeCell3 = 1, kCeTable = 2 };
 
+// Host: whether the float reciprocal division of qdiv is exact for divisor d
+// (exhaustive check over all significands; defined in engine.cu).
+bool host_recip_division_exact(float d);
+
 }  // namespace pfb

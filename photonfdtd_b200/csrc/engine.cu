@@ -639,6 +639,10 @@ bool valid_comp(int c) { return c >= 0 && c < 6; }
 
 }  // namespace
 
+namespace pfb {
+bool host_recip_division_exact(float d) { return recip_division_exact(d); }
+}  // namespace pfb
+
 // ===========================================================================
 // C ABI
 // ===========================================================================

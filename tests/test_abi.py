@@ -16,13 +16,13 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def header_symbols():
     src = open(os.path.join(ROOT, "include", "pfb200.h")).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(pf_[a-z_]+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(pfb?_[a-z_]+)\s*\(", src)))
 
 
 def test_library_exports_every_declared_symbol():
     lib = N.lib()
     syms = header_symbols()
-    assert len(syms) >= 19
+    assert len(syms) >= 19 + 15
     for s in syms:
         assert hasattr(lib, s), f"{s} declared in include/pfb200.h but not exported"
         assert s in N.SIGNATURES, f"{s} has no ctypes signature"
@@ -59,3 +59,18 @@ def test_check_maps_codes_to_python_errors():
         N.check(N.PF_ERR_UNSUPPORTED, None)
     with pytest.raises(N.NativeError):
         N.check(N.PF_ERR_CUDA, None)
+
+
+def test_batch_rejects_bad_arguments_and_null_handles():
+    lib = N.lib()
+    h = C.c_void_p()
+    for args in ((0, 4), (2, 3)):
+        assert lib.pfb_create(*args, 1.0, 1.0, 1.0, 1.0, 10, C.byref(h)) == N.PF_ERR_INVALID
+        assert h.value is None
+    assert lib.pfb_create(2, 4, 1.0, 1.0, 1.0, 1.0, 0, C.byref(h)) == N.PF_ERR_INVALID
+    assert lib.pfb_forward(None) == N.PF_ERR_INVALID
+    assert lib.pfb_adjoint(None, None) == N.PF_ERR_INVALID
+    assert lib.pfb_finalize(None, 8, 8) == N.PF_ERR_INVALID
+    assert lib.pfb_read_dft(None, None) == N.PF_ERR_INVALID
+    assert lib.pfb_last_error(None).decode()
+    lib.pfb_destroy(None)
