@@ -259,7 +259,8 @@ int pfb_set_dft(pf_batch *b, int n_freq, const double *phase);
 /* Lays out the pooled arrays and uploads everything. checkpoint_every = K:
  * the state is stored every K steps (ceil(n_steps/K) - 1 states), and the
  * adjoint replays K steps at a time; K >= n_steps stores no state and needs
- * no replay. tile_rows: x rows per 32-wide tile (4, 8 or 16). */
+ * no replay. tile_rows: x rows per 32-wide tile (8, 16 or 32; a thread
+ * updates tile_rows / 8 consecutive rows). */
 int pfb_finalize(pf_batch *b, int checkpoint_every, int tile_rows);
 
 /* Replaces the design-window coefficients of every instance from a packed

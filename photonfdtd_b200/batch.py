@@ -157,7 +157,7 @@ class BatchTE:
     """
 
     def __init__(self, sims: Sequence, windows: Sequence[Tuple[int, int, int]],
-                 checkpoint_every: Optional[int] = None, tile_rows: int = 8):
+                 checkpoint_every: Optional[int] = None, tile_rows: int = 32):
         if len(sims) == 0 or len(sims) != len(windows):
             raise ValueError("need one design window per simulation")
         wave_cache: Dict = {}

@@ -1,17 +1,19 @@
 // batch2d.cu - batched 2D TE engine with a hand-written discrete adjoint.
 //
 // Many uneven 2D instances (xy plane, nz = 1) are stepped together. Their
-// fields live in pooled arrays, and every kernel walks one work list of
-// 32 (y) x TI (x) tiles drawn from all instances (grid-stride, so one launch
-// covers the batch whatever the sizes). Only Ex, Ey, Hz are stepped: with
-// TE-only sources the other three components of the reference's update
+// fields live in pooled arrays (rows padded to a 32-cell pitch), and every
+// kernel walks one work list of tiles drawn from all instances
+// (batch2d_kernels.cuh). Only Ex, Ey, Hz are stepped: with TE-only sources
+// the other three components of the reference's update
 // (src/photonfdtd/simulation.py:1252-1309 with nz = 1) stay exactly zero, so
-// Ex, Ey, Hz are the reference's to the bit. The step index lives in device
-// memory; chunks of steps are captured once as CUDA graphs and replayed.
+// Ex, Ey, Hz are the reference's to the bit. Chunks of steps are captured
+// once as CUDA graphs and replayed; the chunk's first step lives in device
+// memory.
 //
 // Step n: Hz (curl of E, CPML psi along x and y), H sources, Ex / Ey (curl
 // of Hz, psi), E sources, the output-line DFT of Ey accumulated in
-// complex128: acc += (exp(i w (n+1) dt) * Ey) * dt.
+// complex128: acc += (exp(i w (n+1) dt) * Ey) * dt (samples kept in a ring
+// and folded in step order every 32 steps).
 //
 // The adjoint is the transpose of that (affine) step, applied backward in
 // time. For a real loss L of the line DFT F, the caller passes the
@@ -25,7 +27,7 @@
 // start of every K-step segment; the adjoint replays each earlier segment from
 // its checkpoint to refill the ring, then runs its K transposed steps. The
 // last segment's ring is left by the forward run itself. Memory is
-// ceil(N / K) states + K window rings; K >= N keeps one state and needs no
+// ceil(N / K) - 1 states + K window rings; K >= N keeps no state and needs no
 // replay.
 #include <algorithm>
 #include <cstdarg>
@@ -38,320 +40,12 @@
 #include <vector>
 
 #include "../../include/pfb200.h"
+#include "batch2d_kernels.cuh"
 #include "common.cuh"
 
 using namespace pfb;
+using namespace pfb::b2d;
 
-namespace {
-
-struct Inst {
-  int nx, ny;
-  long long off;                         // first cell in the pooled field arrays
-  int ox, oy;                            // first entry in the pooled x / y coefficients
-  long long p_hzx, p_hzy, p_exy, p_eyx;  // first element of each psi array
-  int nphx, nphy, npex, npey;            // compact psi extents along their axes
-  int di0, dj0, dn;                      // design window
-  long long goff;                        // first design cell (dn * dn per instance)
-  int line_i;                            // x index of the output line
-  long long loff;                        // first line cell (ny per instance)
-};
-
-template <typename T>
-struct BArgs {
-  const Inst* inst;
-  const int4* tiles;  // (instance, i0, j0, -)
-  int ntiles;
-  T *Ex, *Ey, *Hz;
-  const T* ce;
-  const T *bex, *cex, *bhx, *chx, *bey, *cey, *bhy, *chy;
-  const int *mex, *mhx, *mey, *mhy;
-  T *pHzx, *pHzy, *pExy, *pEyx;
-  T dx, dy, rdx, rdy, ch;
-  T idx, idy;  // 1/dx, 1/dy rounded once (adjoint kernels only)
-  bool fdx, fdy;
-};
-
-// ---- forward ---------------------------------------------------------------
-// Hz^{n+1/2} = Hz - ch (dEy/dx - dEx/dy) - ch psi_x + ch psi_y, where the
-// forward differences exist (i < nx-1, j < ny-1).
-template <typename T, int TI>
-__global__ void __launch_bounds__(32 * TI) kb_h(const __grid_constant__ BArgs<T> a) {
-  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-    const int4 tl = a.tiles[t];
-    const Inst& I = a.inst[tl.x];
-    const int i = tl.y + threadIdx.y, j = tl.z + threadIdx.x;
-    if (i >= I.nx - 1 || j >= I.ny - 1) continue;
-    const long long id = I.off + (long long)i * I.ny + j;
-    const T ey = a.Ey[id], ex = a.Ex[id];
-    const T dA = qdiv(sub_rn(a.Ey[id + I.ny], ey), a.dx, a.rdx, a.fdx);
-    const T dB = qdiv(sub_rn(a.Ex[id + 1], ex), a.dy, a.rdy, a.fdy);
-    const T mch = -a.ch;
-    T h = add_rn(a.Hz[id], mul_rn(sub_rn(dA, dB), mch));
-    const int mx = a.mhx[I.ox + i];
-    if (mx >= 0) {
-      const long long q = I.p_hzx + (long long)mx * I.ny + j;
-      const T psi = add_rn(mul_rn(a.bhx[I.ox + i], a.pHzx[q]), mul_rn(a.chx[I.ox + i], dA));
-      a.pHzx[q] = psi;
-      h = add_rn(h, mul_rn(mch, psi));
-    }
-    const int my = a.mhy[I.oy + j];
-    if (my >= 0) {
-      const long long q = I.p_hzy + (long long)i * I.nphy + my;
-      const T psi = add_rn(mul_rn(a.bhy[I.oy + j], a.pHzy[q]), mul_rn(a.chy[I.oy + j], dB));
-      a.pHzy[q] = psi;
-      h = add_rn(h, mul_rn(a.ch, psi));
-    }
-    a.Hz[id] = h;
-  }
-}
-
-// Ex^{n+1} = Ex + K dHz/dy + K psi_y (j >= 1); Ey^{n+1} = Ey - K dHz/dx -
-// K psi_x (i >= 1). With `ring`, design cells store the curls that
-// multiplied K: ring[n mod K][cell] = (cEx, cEy).
-template <typename T, int TI>
-__global__ void __launch_bounds__(32 * TI) kb_e(const __grid_constant__ BArgs<T> a, T* ring,
-                                               long long n_design, const long long* step,
-                                               int ring_len) {
-  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-    const int4 tl = a.tiles[t];
-    const Inst& I = a.inst[tl.x];
-    const int i = tl.y + threadIdx.y, j = tl.z + threadIdx.x;
-    if (i >= I.nx || j >= I.ny) continue;
-    const long long id = I.off + (long long)i * I.ny + j;
-    const T K = a.ce[id];
-    const T hz = a.Hz[id];
-    T cx = T(0), cy = T(0);
-    if (j >= 1) {
-      const T dA = qdiv(sub_rn(hz, a.Hz[id - 1]), a.dy, a.rdy, a.fdy);
-      T e = add_rn(a.Ex[id], mul_rn(dA, K));
-      cx = dA;
-      const int my = a.mey[I.oy + j];
-      if (my >= 0) {
-        const long long q = I.p_exy + (long long)i * I.npey + my;
-        const T psi = add_rn(mul_rn(a.bey[I.oy + j], a.pExy[q]), mul_rn(a.cey[I.oy + j], dA));
-        a.pExy[q] = psi;
-        e = add_rn(e, mul_rn(K, psi));
-        cx = add_rn(dA, psi);
-      }
-      a.Ex[id] = e;
-    }
-    if (i >= 1) {
-      const T dB = qdiv(sub_rn(hz, a.Hz[id - I.ny]), a.dx, a.rdx, a.fdx);
-      T e = add_rn(a.Ey[id], mul_rn(-dB, K));
-      cy = -dB;
-      const int mx = a.mex[I.ox + i];
-      if (mx >= 0) {
-        const long long q = I.p_eyx + (long long)mx * I.ny + j;
-        const T psi = add_rn(mul_rn(a.bex[I.ox + i], a.pEyx[q]), mul_rn(a.cex[I.ox + i], dB));
-        a.pEyx[q] = psi;
-        e = add_rn(e, mul_rn(-K, psi));
-        cy = sub_rn(cy, psi);
-      }
-      a.Ey[id] = e;
-    }
-    if (ring) {
-      const int di = i - I.di0, dj = j - I.dj0;
-      if (di >= 0 && di < I.dn && dj >= 0 && dj < I.dn) {
-        const long long slot = *step % ring_len;
-        T* r = ring + (slot * n_design + I.goff + (long long)di * I.dn + dj) * 2;
-        r[0] = cx;
-        r[1] = cy;
-      }
-    }
-  }
-}
-
-struct BSources {
-  const long long* cell;  // pooled cell of each group
-  const int* comp;        // 0 Ex, 1 Ey, 2 Hz
-  const int* start;       // group q owns entries start[q] .. start[q+1]-1
-  const int* wave_row;
-  const double* amp;
-  const double* wave;     // (rows, n_steps) waveform values at the family's times
-  long long n_steps;
-  int n_groups;
-};
-
-// Soft sources: field += amp * waveform, in list order per cell, each term
-// added in double and rounded once (numpy's array += python float).
-template <typename T>
-__global__ void kb_inject(BSources s, T* Ex, T* Ey, T* Hz, int family_h, const long long* step) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= s.n_groups) return;
-  const int c = s.comp[g];
-  if ((c == 2) != (family_h != 0)) return;
-  T* F = c == 0 ? Ex : (c == 1 ? Ey : Hz);
-  const long long n = *step;
-  T v = F[s.cell[g]];
-  for (int q = s.start[g]; q < s.start[g + 1]; ++q)
-    v = add_double<T>(v, __dmul_rn(s.amp[q], s.wave[(long long)s.wave_row[q] * s.n_steps + n]));
-  F[s.cell[g]] = v;
-}
-
-// Line DFT of Ey in the reference's order: acc += (phase * Ey) * dt, per step.
-template <typename T>
-__global__ void kb_dft(const long long* lcell, long long nline, const T* Ey, double* acc,
-                       const double* phase, int n_freq, double dt, const long long* step) {
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nline) return;
-  const double s = (double)Ey[lcell[c]];
-  const double* ph = phase + (*step) * n_freq * 2;
-  double* A = acc + c * n_freq * 2;
-  for (int f = 0; f < n_freq; ++f) {
-    A[2 * f] = __dadd_rn(A[2 * f], __dmul_rn(__dmul_rn(ph[2 * f], s), dt));
-    A[2 * f + 1] = __dadd_rn(A[2 * f + 1], __dmul_rn(__dmul_rn(ph[2 * f + 1], s), dt));
-  }
-}
-
-__global__ void kb_tick(long long* step, long long by) { *step += by; }
-__global__ void kb_set(long long* step, long long v) { *step = v; }
-
-// Writes packed design-window coefficients into the pooled ce array.
-template <typename T>
-__global__ void kb_scatter_design(const Inst* inst, int n_inst, const T* src, T* ce) {
-  const int k = blockIdx.y;
-  if (k >= n_inst) return;
-  const Inst& I = inst[k];
-  const int n = I.dn * I.dn;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-    const int di = q / I.dn, dj = q % I.dn;
-    ce[I.off + (long long)(I.di0 + di) * I.ny + I.dj0 + dj] = src[I.goff + q];
-  }
-}
-
-// ---- adjoint ---------------------------------------------------------------
-template <typename T>
-struct AArgs {
-  T *aEx, *aEy, *aHz, *aHzx, *aHzy, *aExy, *aEyx;  // adjoint state
-  T *gA, *gB, *hA, *hB;                             // adjoints of the per-cell differences
-  double* grad;                                     // dL/dK per design cell
-  const T* ring;                                    // forward curls, slot = n mod K
-  long long n_design;
-  int ring_len;
-};
-
-// Adjoint source of step n on the output line.
-template <typename T>
-__global__ void kb_adj_src(const long long* lcell, long long nline, T* aEy, const double* G,
-                           const double* phase, int n_freq, double dt, const long long* step) {
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nline) return;
-  const double* ph = phase + (*step) * n_freq * 2;
-  const double* g = G + c * n_freq * 2;
-  double s = 0.0;
-  for (int f = 0; f < n_freq; ++f) s += g[2 * f] * ph[2 * f] + g[2 * f + 1] * ph[2 * f + 1];
-  const long long id = lcell[c];
-  aEy[id] = (T)((double)aEy[id] + dt * s);
-}
-
-// Transpose of the E update of step n (cell-local): the K gradient, the E psi
-// adjoints, gA = adjoint of dHz/dy in Ex, gB = adjoint of dHz/dx in Ey.
-template <typename T, int TI>
-__global__ void __launch_bounds__(32 * TI) kb_adj_e(const __grid_constant__ BArgs<T> a,
-                                                   const __grid_constant__ AArgs<T> d,
-                                                   const long long* step) {
-  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-    const int4 tl = a.tiles[t];
-    const Inst& I = a.inst[tl.x];
-    const int i = tl.y + threadIdx.y, j = tl.z + threadIdx.x;
-    if (i >= I.nx || j >= I.ny) continue;
-    const long long id = I.off + (long long)i * I.ny + j;
-    const T K = a.ce[id];
-    const T lx = d.aEx[id], ly = d.aEy[id];
-    const int di = i - I.di0, dj = j - I.dj0;
-    if (di >= 0 && di < I.dn && dj >= 0 && dj < I.dn) {
-      const long long dc = I.goff + (long long)di * I.dn + dj;
-      const T* r = d.ring + ((*step % d.ring_len) * d.n_design + dc) * 2;
-      d.grad[dc] += (double)lx * (double)r[0] + (double)ly * (double)r[1];
-    }
-    T ga = T(0), gb = T(0);
-    if (j >= 1) {
-      ga = K * lx;
-      const int my = a.mey[I.oy + j];
-      if (my >= 0) {
-        const long long q = I.p_exy + (long long)i * I.npey + my;
-        const T ap = d.aExy[q] + K * lx;
-        ga += a.cey[I.oy + j] * ap;
-        d.aExy[q] = a.bey[I.oy + j] * ap;
-      }
-    }
-    if (i >= 1) {
-      gb = -K * ly;
-      const int mx = a.mex[I.ox + i];
-      if (mx >= 0) {
-        const long long q = I.p_eyx + (long long)mx * I.ny + j;
-        const T ap = d.aEyx[q] - K * ly;
-        gb += a.cex[I.ox + i] * ap;
-        d.aEyx[q] = a.bex[I.ox + i] * ap;
-      }
-    }
-    d.gA[id] = ga;
-    d.gB[id] = gb;
-  }
-}
-
-// Transpose of the H update: gathers the E-update terms into aHz, then the H
-// psi adjoints and hA = adjoint of dEy/dx, hB = adjoint of dEx/dy.
-template <typename T, int TI>
-__global__ void __launch_bounds__(32 * TI) kb_adj_h(const __grid_constant__ BArgs<T> a,
-                                                   const __grid_constant__ AArgs<T> d) {
-  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-    const int4 tl = a.tiles[t];
-    const Inst& I = a.inst[tl.x];
-    const int i = tl.y + threadIdx.y, j = tl.z + threadIdx.x;
-    if (i >= I.nx || j >= I.ny) continue;
-    const long long id = I.off + (long long)i * I.ny + j;
-    T ah = d.aHz[id];
-    T ga = d.gA[id], gb = d.gB[id];
-    if (j + 1 < I.ny) ga -= d.gA[id + 1];
-    if (i + 1 < I.nx) gb -= d.gB[id + I.ny];
-    ah += ga * a.idy + gb * a.idx;
-    T ha = T(0), hb = T(0);
-    if (i < I.nx - 1 && j < I.ny - 1) {
-      ha = -a.ch * ah;
-      hb = a.ch * ah;
-      const int mx = a.mhx[I.ox + i];
-      if (mx >= 0) {
-        const long long q = I.p_hzx + (long long)mx * I.ny + j;
-        const T ap = d.aHzx[q] - a.ch * ah;
-        ha += a.chx[I.ox + i] * ap;
-        d.aHzx[q] = a.bhx[I.ox + i] * ap;
-      }
-      const int my = a.mhy[I.oy + j];
-      if (my >= 0) {
-        const long long q = I.p_hzy + (long long)i * I.nphy + my;
-        const T ap = d.aHzy[q] + a.ch * ah;
-        hb += a.chy[I.oy + j] * ap;
-        d.aHzy[q] = a.bhy[I.oy + j] * ap;
-      }
-    }
-    d.aHz[id] = ah;
-    d.hA[id] = ha;
-    d.hB[id] = hb;
-  }
-}
-
-// E adjoints from the H update's differences (gathered from i-1 / j-1).
-template <typename T, int TI>
-__global__ void __launch_bounds__(32 * TI) kb_adj_e2(const __grid_constant__ BArgs<T> a,
-                                                    const __grid_constant__ AArgs<T> d) {
-  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
-    const int4 tl = a.tiles[t];
-    const Inst& I = a.inst[tl.x];
-    const int i = tl.y + threadIdx.y, j = tl.z + threadIdx.x;
-    if (i >= I.nx || j >= I.ny) continue;
-    const long long id = I.off + (long long)i * I.ny + j;
-    T ha = -d.hA[id], hb = -d.hB[id];
-    if (i >= 1) ha += d.hA[id - I.ny];
-    if (j >= 1) hb += d.hB[id - 1];
-    d.aEy[id] += ha * a.idx;
-    d.aEx[id] += hb * a.idy;
-  }
-}
-
-}  // namespace
-
-// ===========================================================================
 struct pf_batch {
   int n_inst = 0, rb = 4;
   double dx = 1, dy = 1, ch = 0, dt = 0;
@@ -361,10 +55,12 @@ struct pf_batch {
   std::vector<Inst> inst;
   std::vector<std::vector<char>> h_ce;
   std::vector<std::vector<char>> h_coef[8];  // bex cex bhx chx bey cey bhy chy
-  long long ncell = 0, nx_tot = 0, ny_tot = 0, n_design = 0, nline = 0;
+  long long ncell = 0, ncell_real = 0, nx_tot = 0, ny_tot = 0, n_design = 0, nline = 0;
   long long npsi[4] = {};
-  int ti = 8;
+  int rows = 4;  // rows per thread (tile = 32 columns x 8 * rows)
   int ckpt = 64;
+  bool merge_post = true;  // no E-source group sits on an output-line cell
+  int n_h_groups = 0;      // source groups on Hz
   bool finalized = false, fwd_done = false, ring_last = false;
   bool fd[2] = {false, false};
   double rd[2] = {1, 1};
@@ -375,7 +71,7 @@ struct pf_batch {
   // device
   std::vector<void*> allocs;
   Inst* d_inst = nullptr;
-  int4* d_tiles = nullptr;
+  TileRec* d_tiles = nullptr;
   int ntiles = 0;
   void *Ex = nullptr, *Ey = nullptr, *Hz = nullptr, *ce = nullptr;
   void* coef[8] = {};
@@ -393,11 +89,13 @@ struct pf_batch {
   double* cot = nullptr;
   long long* lcell = nullptr;
   double* phase = nullptr;
-  long long* step = nullptr;
+  long long* base = nullptr;  // first step of the running chunk
+  void* dring = nullptr;      // DFT line samples, kDftRing x line cells
   BSources src{};
-  // instantiated graphs, keyed by (chunk kind, steps)
-  std::map<std::pair<int, long long>, cudaGraphExec_t> graphs;
+  // instantiated graphs and their kernel counts, keyed by (chunk kind, steps)
+  std::map<std::pair<int, long long>, std::pair<cudaGraphExec_t, long long>> graphs;
   int64_t launches = 0;
+  long long capture_launches = 0;
 };
 
 namespace {
@@ -469,6 +167,10 @@ BArgs<T> bargs(pf_batch* b) {
   a.ch = (T)b->ch;
   a.idx = (T)(1.0 / b->dx);
   a.idy = (T)(1.0 / b->dy);
+  a.base = b->base;
+  a.ring = (T*)b->ring;
+  a.n_design = b->n_design;
+  a.ring_len = b->ckpt;
   return a;
 }
 
@@ -487,96 +189,126 @@ AArgs<T> aargs(pf_batch* b) {
   d.hA = (T*)b->g[2];
   d.hB = (T*)b->g[3];
   d.grad = b->grad;
-  d.ring = (const T*)b->ring;
-  d.n_design = b->n_design;
-  d.ring_len = b->ckpt;
+  d.cot = b->cot;
+  d.phase = b->phase;
+  d.n_freq = b->n_freq;
+  d.dt = b->dt;
   return d;
 }
 
-// Persistent-style grid: as many blocks as fit on the 148 SMs walk the tiles.
-int grid_blocks(const pf_batch* b) {
-  return std::max(1, std::min(b->ntiles, 148 * (2048 / (32 * b->ti))));
-}
+// One tile per block (the kernels also accept a smaller grid).
+int grid_blocks(const pf_batch* b) { return std::max(1, b->ntiles); }
 
-template <typename T, int TI>
-void fwd_kernels(pf_batch* b, bool dft, bool record) {
+template <typename T, int R>
+void fwd_kernels(pf_batch* b, long long len, bool dft) {
   const BArgs<T> a = bargs<T>(b);
-  const dim3 blk(32, TI);
+  const dim3 blk(32, kWarps);
   const int G = grid_blocks(b);
-  kb_h<T, TI><<<G, blk, 0, b->stream>>>(a);
-  if (b->src.n_groups)
-    kb_inject<T><<<(b->src.n_groups + 127) / 128, 128, 0, b->stream>>>(b->src, a.Ex, a.Ey, a.Hz, 1,
-                                                                         b->step);
-  kb_e<T, TI><<<G, blk, 0, b->stream>>>(a, record ? (T*)b->ring : nullptr, b->n_design, b->step,
-                                        b->ckpt);
-  if (b->src.n_groups)
-    kb_inject<T><<<(b->src.n_groups + 127) / 128, 128, 0, b->stream>>>(b->src, a.Ex, a.Ey, a.Hz, 0,
-                                                                         b->step);
-  if (dft && b->nline)
-    kb_dft<T><<<(unsigned)((b->nline + 127) / 128), 128, 0, b->stream>>>(
-        b->lcell, b->nline, a.Ey, b->acc, b->phase, b->n_freq, b->dt, b->step);
-  kb_tick<<<1, 1, 0, b->stream>>>(b->step, 1);
+  const long long ng = b->src.n_groups;
+  int pend = 0;
+  for (long long t = 0; t < len; ++t) {
+    if (b->n_h_groups) {
+      kb_post<T><<<(unsigned)((ng + 127) / 128), 128, 0, b->stream>>>(
+          b->src, a.Ex, a.Ey, a.Hz, 1, b->base, (int)t, b->lcell, 0, (T*)nullptr);
+      ++b->capture_launches;
+    }
+    kb_h<T, R><<<G, blk, 0, b->stream>>>(a);
+    kb_e<T, R><<<G, blk, 0, b->stream>>>(a, (int)t);
+    b->capture_launches += 2;
+    T* dring = dft ? (T*)b->dring : nullptr;
+    if (b->merge_post || !dft) {
+      const long long n = ng + (dft ? b->nline : 0);
+      if (n) {
+        kb_post<T><<<(unsigned)((n + 127) / 128), 128, 0, b->stream>>>(
+            b->src, a.Ex, a.Ey, a.Hz, 0, b->base, (int)t, b->lcell, b->nline, dring);
+        ++b->capture_launches;
+      }
+    } else {
+      if (ng) {
+        kb_post<T><<<(unsigned)((ng + 127) / 128), 128, 0, b->stream>>>(
+            b->src, a.Ex, a.Ey, a.Hz, 0, b->base, (int)t, b->lcell, 0, (T*)nullptr);
+        ++b->capture_launches;
+      }
+      BSources none = b->src;
+      none.n_groups = 0;
+      kb_post<T><<<(unsigned)((b->nline + 127) / 128), 128, 0, b->stream>>>(
+          none, a.Ex, a.Ey, a.Hz, 0, b->base, (int)t, b->lcell, b->nline, dring);
+      ++b->capture_launches;
+    }
+    if (dft) {
+      ++pend;
+      if (pend == kDftRing || t + 1 == len) {
+        const long long n = b->nline * b->n_freq;
+        kb_dft_flush<T><<<(unsigned)((n + 255) / 256), 256, 0, b->stream>>>(
+            (const T*)b->dring, b->nline, b->acc, b->phase, b->n_freq, b->dt, b->base,
+            (int)(t + 1 - pend), pend);
+        ++b->capture_launches;
+        pend = 0;
+      }
+    }
+  }
 }
 
-template <typename T>
-void fwd_step(pf_batch* b, bool dft, bool record) {
-  if (b->ti == 4) fwd_kernels<T, 4>(b, dft, record);
-  else if (b->ti == 8) fwd_kernels<T, 8>(b, dft, record);
-  else fwd_kernels<T, 16>(b, dft, record);
-}
-
-template <typename T, int TI>
-void adj_kernels(pf_batch* b) {
+// Reverse pass over chunk steps len-1 .. 0 (n = *base + t): the E transpose
+// of the top step, then per step the H transpose and a cell pass that
+// finishes that step's E adjoints and, except after the lowest step (whose
+// predecessor belongs to the previous segment), runs the next lower step's E
+// transpose.
+template <typename T, int R>
+void adj_kernels(pf_batch* b, long long len) {
   const BArgs<T> a = bargs<T>(b);
   const AArgs<T> d = aargs<T>(b);
-  const dim3 blk(32, TI);
+  const dim3 blk(32, kWarps);
   const int G = grid_blocks(b);
-  if (b->nline)
-    kb_adj_src<T><<<(unsigned)((b->nline + 127) / 128), 128, 0, b->stream>>>(
-        b->lcell, b->nline, d.aEy, b->cot, b->phase, b->n_freq, b->dt, b->step);
-  kb_adj_e<T, TI><<<G, blk, 0, b->stream>>>(a, d, b->step);
-  kb_adj_h<T, TI><<<G, blk, 0, b->stream>>>(a, d);
-  kb_adj_e2<T, TI><<<G, blk, 0, b->stream>>>(a, d);
-  kb_tick<<<1, 1, 0, b->stream>>>(b->step, -1);
+  kb_adj_cell<T, R, false, true><<<G, blk, 0, b->stream>>>(a, d, (int)(len - 1));
+  for (long long t = len - 1; t >= 0; --t) {
+    kb_adj_h<T, R><<<G, blk, 0, b->stream>>>(a, d);
+    if (t > 0)
+      kb_adj_cell<T, R, true, true><<<G, blk, 0, b->stream>>>(a, d, (int)(t - 1));
+    else
+      kb_adj_cell<T, R, true, false><<<G, blk, 0, b->stream>>>(a, d, 0);
+  }
+  b->capture_launches += 1 + 2 * len;
 }
 
 template <typename T>
-void adj_step(pf_batch* b) {
-  if (b->ti == 4) adj_kernels<T, 4>(b);
-  else if (b->ti == 8) adj_kernels<T, 8>(b);
-  else adj_kernels<T, 16>(b);
-}
-
-// Kernel launches of one step of each chunk kind.
-long long launches_per_step(const pf_batch* b, int kind) {
-  if (kind == 2) return 4 + (b->nline ? 1 : 0);
-  return 3 + (b->src.n_groups ? 2 : 0) + (kind == 0 && b->nline ? 1 : 0);
+void chunk_kernels(pf_batch* b, int kind, long long len) {
+  if (kind == 2) {
+    if (b->rows == 1) adj_kernels<T, 1>(b, len);
+    else if (b->rows == 2) adj_kernels<T, 2>(b, len);
+    else adj_kernels<T, 4>(b, len);
+  } else {
+    if (b->rows == 1) fwd_kernels<T, 1>(b, len, kind == 0);
+    else if (b->rows == 2) fwd_kernels<T, 2>(b, len, kind == 0);
+    else fwd_kernels<T, 4>(b, len, kind == 0);
+  }
 }
 
 // Runs `len` steps of kind 0 (forward + DFT + ring), 1 (replay: forward +
-// ring) or 2 (adjoint) as one graph launch. Each (kind, len) is captured
-// once; at most two lengths occur per kind (K and the last segment's).
+// ring) or 2 (adjoint) as one graph launch, chunk step t = 0 at *base. Each
+// (kind, len) is captured once; at most two lengths occur per kind (K and
+// the last segment's).
 template <typename T>
 int run_chunk(pf_batch* b, int kind, long long len) {
-  cudaGraphExec_t& ex = b->graphs[std::make_pair(kind, len)];
-  if (ex == nullptr) {
+  if (len > (1LL << 30)) return bfail(b, PF_ERR_INVALID, "chunk too long");
+  auto& ent = b->graphs[std::make_pair(kind, len)];
+  if (ent.first == nullptr) {
     cudaGraph_t graph = nullptr;
     B_CUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    for (long long t = 0; t < len; ++t) {
-      if (kind == 2) adj_step<T>(b);
-      else fwd_step<T>(b, kind == 0, true);
-    }
+    b->capture_launches = 0;
+    chunk_kernels<T>(b, kind, len);
     const cudaError_t e1 = cudaStreamEndCapture(b->stream, &graph);
     if (e1 != cudaSuccess) return bfail(b, PF_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e1));
-    const cudaError_t e2 = cudaGraphInstantiate(&ex, graph, 0);
+    const cudaError_t e2 = cudaGraphInstantiate(&ent.first, graph, 0);
     cudaGraphDestroy(graph);
     if (e2 != cudaSuccess) {
-      ex = nullptr;
+      ent.first = nullptr;
       return bfail(b, PF_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e2));
     }
+    ent.second = b->capture_launches;
   }
-  B_CUDA(b, cudaGraphLaunch(ex, b->stream));
-  b->launches += launches_per_step(b, kind) * len;
+  B_CUDA(b, cudaGraphLaunch(ent.first, b->stream));
+  b->launches += ent.second;
   return PF_OK;
 }
 
@@ -599,8 +331,8 @@ int state_copy(pf_batch* b, long long s, bool save) {
   return PF_OK;
 }
 
-int set_step(pf_batch* b, long long s) {
-  kb_set<<<1, 1, 0, b->stream>>>(b->step, s);
+int set_base(pf_batch* b, long long s) {
+  kb_set<<<1, 1, 0, b->stream>>>(b->base, s);
   b->launches += 1;
   B_CUDA(b, cudaGetLastError());
   return PF_OK;
@@ -619,10 +351,10 @@ int forward_t(pf_batch* b) {
   int rc;
   if ((rc = zero_state(b))) return rc;
   B_CUDA(b, cudaMemsetAsync(b->acc, 0, (size_t)b->nline * b->n_freq * 16, b->stream));
-  if ((rc = set_step(b, 0))) return rc;
   const long long K = b->ckpt;
   for (long long s0 = 0; s0 < b->n_steps; s0 += K) {
     if (s0 > 0 && (rc = state_copy(b, s0 / K - 1, true))) return rc;  // segment 0 starts at zero
+    if ((rc = set_base(b, s0))) return rc;
     if ((rc = run_chunk<T>(b, 0, std::min(K, b->n_steps - s0)))) return rc;
   }
   B_CUDA(b, cudaGetLastError());
@@ -637,8 +369,10 @@ int adjoint_t(pf_batch* b) {
   const size_t S = b->rb;
   int rc;
   for (int q = 0; q < 3; ++q) B_CUDA(b, cudaMemsetAsync(b->aE[q], 0, b->ncell * S, b->stream));
-  for (int q = 0; q < 4; ++q)
+  for (int q = 0; q < 4; ++q) {
     if (b->npsi[q]) B_CUDA(b, cudaMemsetAsync(b->apsi[q], 0, b->npsi[q] * S, b->stream));
+    B_CUDA(b, cudaMemsetAsync(b->g[q], 0, b->ncell * S, b->stream));
+  }
   B_CUDA(b, cudaMemsetAsync(b->grad, 0, (size_t)b->n_design * 8, b->stream));
   const long long K = b->ckpt;
   const long long nseg = (b->n_steps + K - 1) / K;
@@ -650,10 +384,10 @@ int adjoint_t(pf_batch* b) {
       } else if ((rc = state_copy(b, sg - 1, false))) {
         return rc;
       }
-      if ((rc = set_step(b, s0))) return rc;
+      if ((rc = set_base(b, s0))) return rc;
       if ((rc = run_chunk<T>(b, 1, len))) return rc;
     }
-    if ((rc = set_step(b, s0 + len - 1))) return rc;
+    if ((rc = set_base(b, s0))) return rc;
     if ((rc = run_chunk<T>(b, 2, len))) return rc;
   }
   B_CUDA(b, cudaGetLastError());
@@ -666,7 +400,7 @@ int adjoint_t(pf_batch* b) {
 
 void destroy_graphs(pf_batch* b) {
   for (auto& kv : b->graphs)
-    if (kv.second) cudaGraphExecDestroy(kv.second);
+    if (kv.second.first) cudaGraphExecDestroy(kv.second.first);
   b->graphs.clear();
 }
 
@@ -785,21 +519,22 @@ int pfb_finalize(pf_batch* b, int checkpoint_every, int tile_rows) {
   if (!b) return PF_ERR_INVALID;
   if (b->finalized) return bfail(b, PF_ERR_STATE, "pfb_finalize called twice");
   if (checkpoint_every < 1) return bfail(b, PF_ERR_INVALID, "checkpoint_every must be >= 1");
-  if (tile_rows != 4 && tile_rows != 8 && tile_rows != 16)
-    return bfail(b, PF_ERR_INVALID, "tile_rows must be 4, 8 or 16");
+  if (tile_rows != 8 && tile_rows != 16 && tile_rows != 32)
+    return bfail(b, PF_ERR_INVALID, "tile_rows must be 8, 16 or 32");
   if (b->n_freq < 1) return bfail(b, PF_ERR_STATE, "pfb_set_dft must come before pfb_finalize");
   for (int k = 0; k < b->n_inst; ++k)
     if (b->inst[k].nx == 0) return bfail(b, PF_ERR_STATE, "instance %d not set", k);
   b->ckpt = (int)std::min<long long>(checkpoint_every, b->n_steps);
-  b->ti = tile_rows;
+  b->rows = tile_rows / kWarps;
   const size_t S = b->rb;
   std::vector<int> mp[4];
   std::vector<char> coefp[8], cep;
   std::vector<long long> lcell;
-  std::vector<int4> tiles;
+  std::vector<TileRec> tiles;
   for (int k = 0; k < b->n_inst; ++k) {
     Inst& I = b->inst[k];
-    I.off = b->ncell;
+    I.pitch = (I.ny + 31) / 32 * 32;
+    I.off = b->ncell;  // a multiple of 32: every instance holds nx * pitch cells
     I.ox = (int)b->nx_tot;
     I.oy = (int)b->ny_tot;
     I.goff = b->n_design;
@@ -825,13 +560,35 @@ int pfb_finalize(pf_batch* b, int checkpoint_every, int tile_rows) {
     b->npsi[1] += (long long)I.nx * I.nphy;
     b->npsi[2] += (long long)I.nx * I.npey;
     b->npsi[3] += (long long)I.npex * I.ny;
-    cep.insert(cep.end(), b->h_ce[k].begin(), b->h_ce[k].end());
+    {
+      const size_t row = (size_t)I.ny * S, prow = (size_t)I.pitch * S, o = cep.size();
+      cep.resize(o + (size_t)I.nx * prow, 0);
+      for (int i = 0; i < I.nx; ++i)
+        memcpy(cep.data() + o + i * prow, b->h_ce[k].data() + i * row, row);
+    }
     for (int q = 0; q < 8; ++q)
       coefp[q].insert(coefp[q].end(), b->h_coef[q][k].begin(), b->h_coef[q][k].end());
-    for (int j = 0; j < I.ny; ++j) lcell.push_back(I.off + (long long)I.line_i * I.ny + j);
-    for (int i0 = 0; i0 < I.nx; i0 += b->ti)
-      for (int j0 = 0; j0 < I.ny; j0 += 32) tiles.push_back(make_int4(k, i0, j0, 0));
-    b->ncell += (long long)I.nx * I.ny;
+    for (int j = 0; j < I.ny; ++j) lcell.push_back(I.off + (long long)I.line_i * I.pitch + j);
+    for (int i0 = 0; i0 < I.nx; i0 += tile_rows)
+      for (int j0 = 0; j0 < I.ny; j0 += 32) {
+        TileRec tr;
+        tr.base = I.off + (long long)i0 * I.pitch + j0;
+        tr.nx = I.nx;
+        tr.ny = I.ny;
+        tr.pitch = I.pitch;
+        tr.i0 = i0;
+        tr.j0 = j0;
+        tr.ox = I.ox + i0;
+        tr.oy = I.oy + j0;
+        tr.k = k;
+        tr.wdi = I.di0 - i0;
+        tr.wdj = I.dj0 - j0;
+        tr.wdn = I.dn;
+        tr.pad[0] = 0;
+        tiles.push_back(tr);
+      }
+    b->ncell += (long long)I.nx * I.pitch;
+    b->ncell_real += (long long)I.nx * I.ny;
     b->nx_tot += I.nx;
     b->ny_tot += I.ny;
     b->n_design += (long long)I.dn * I.dn;
@@ -842,7 +599,7 @@ int pfb_finalize(pf_batch* b, int checkpoint_every, int tile_rows) {
   b->ntiles = (int)tiles.size();
   int rc;
   if ((rc = bup(b, (void**)&b->d_inst, b->inst.data(), b->inst.size() * sizeof(Inst)))) return rc;
-  if ((rc = bup(b, (void**)&b->d_tiles, tiles.data(), tiles.size() * sizeof(int4)))) return rc;
+  if ((rc = bup(b, (void**)&b->d_tiles, tiles.data(), tiles.size() * sizeof(TileRec)))) return rc;
   if ((rc = bup(b, &b->ce, cep.data(), cep.size()))) return rc;
   for (int q = 0; q < 8; ++q)
     if ((rc = bup(b, &b->coef[q], coefp[q].data(), coefp[q].size()))) return rc;
@@ -868,8 +625,23 @@ int pfb_finalize(pf_batch* b, int checkpoint_every, int tile_rows) {
   if ((rc = balloc(b, (void**)&b->cot, (size_t)b->nline * b->n_freq * 16))) return rc;
   if ((rc = bup(b, (void**)&b->lcell, lcell.data(), lcell.size() * 8))) return rc;
   if ((rc = bup(b, (void**)&b->phase, b->h_phase.data(), b->h_phase.size() * 8))) return rc;
-  if ((rc = balloc(b, (void**)&b->step, 8))) return rc;
-  for (auto& c : b->s_cell) c = b->inst[(int)(c >> 32)].off + (c & 0xffffffffLL);
+  if ((rc = balloc(b, (void**)&b->base, 8))) return rc;
+  if ((rc = balloc(b, &b->dring, (size_t)kDftRing * b->nline * S))) return rc;
+  // one launch may inject E sources and sample the lines only if no E group
+  // sits on a line cell
+  b->merge_post = true;
+  b->n_h_groups = 0;
+  for (size_t q = 0; q < b->s_cell.size(); ++q) {
+    const Inst& I = b->inst[(int)(b->s_cell[q] >> 32)];
+    const long long local = b->s_cell[q] & 0xffffffffLL;
+    if (b->s_comp[q] == 2) ++b->n_h_groups;
+    else if (local / I.ny == I.line_i) b->merge_post = false;
+  }
+  for (auto& c : b->s_cell) {
+    const Inst& I = b->inst[(int)(c >> 32)];
+    const long long local = c & 0xffffffffLL;
+    c = I.off + local / I.ny * I.pitch + local % I.ny;
+  }
   b->src.n_groups = (int)b->s_cell.size();
   b->src.n_steps = b->n_steps;
   if (b->src.n_groups) {
@@ -954,15 +726,16 @@ int pfb_read_field(pf_batch* b, int k, int comp, void* dst) {
     return bfail(b, PF_ERR_INVALID, "bad pfb_read_field");
   const Inst& I = b->inst[k];
   void* src = comp == 0 ? b->Ex : (comp == 1 ? b->Ey : b->Hz);
-  B_CUDA(b, cudaMemcpyAsync(dst, (char*)src + I.off * b->rb, (size_t)I.nx * I.ny * b->rb,
-                            cudaMemcpyDeviceToHost, b->stream));
+  B_CUDA(b, cudaMemcpy2DAsync(dst, (size_t)I.ny * b->rb, (char*)src + I.off * b->rb,
+                              (size_t)I.pitch * b->rb, (size_t)I.ny * b->rb, I.nx,
+                              cudaMemcpyDeviceToHost, b->stream));
   B_CUDA(b, cudaStreamSynchronize(b->stream));
   return PF_OK;
 }
 
 int pfb_info(const pf_batch* b, int64_t* out, int n_out) {
   if (!b || !out) return PF_ERR_INVALID;
-  const int64_t v[8] = {b->ncell,
+  const int64_t v[8] = {b->ncell_real,
                         b->nline,
                         b->n_design,
                         b->ntiles,

@@ -76,7 +76,7 @@ def test_checkpoint_spacing_changes_nothing():
     sims, _, wins = _sims("float64", 200)
     outs = []
     for K in (1, 7, 64, 200, 1000):
-        b = BatchTE(sims, wins, checkpoint_every=K, tile_rows=(4, 8, 16)[K % 3])
+        b = BatchTE(sims, wins, checkpoint_every=K, tile_rows=(8, 16, 32)[K % 3])
         try:
             F = b.forward()
             g1 = b.adjoint(objective_cotangent(F))
