@@ -17,6 +17,13 @@ timed with CUDA events on the engine's stream (max over ranks). With N > 1
 every rank steps its own replica of the workload (the single-domain path
 does not shard; replicas only), so scaling is weak.
 
+The line's "adjoint" object is the second half of the headline metric:
+seconds per gradient iteration of the batched 2D TE inverse-design workload
+(config 4: 256 uneven instances, 4000 steps, 64 x 64 design windows),
+measured through photonfdtd_b200.batch.value_and_grad_eps (host design in,
+host gradient out), with its forward / adjoint split and a CPU baseline of the
+NumPy forward + adjoint restatement on one instance.
+
 --impl reference times the reference's CPU algorithm for the same workload:
 the NumPy restatement in oracle/ (the reference package itself is Python
 and not present where this runs), on a bounded sample of full-domain steps.
@@ -54,6 +61,8 @@ def parse():
     p.add_argument("--size", type=int, default=384, help="cells per axis (default 384)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--adjoint-iters", type=int, default=2)
     return p.parse_args()
 
 
@@ -211,6 +220,71 @@ def run_reference(args):
 
 
 # --------------------------------------------------------------------------- #
+ADJ_WORKLOAD = ("config4: 256 2D TE instances, nx ~U{200..800} x ny ~U{150..400} at 20 nm "
+                "(12-cell CPML), float32, 64x64 design window each, Ey line source, Ey DFT at "
+                "8 wavelengths on the output line, 4000 steps forward + discrete adjoint")
+
+
+def adjoint_bench(iters: int, cpu: bool):
+    """Seconds per gradient iteration of the config-4 batch: set the design,
+    forward, read the line DFT, cotangent of J = sum |F|^2, adjoint, read
+    dJ/deps - one value_and_grad_eps call, wall clock on the host."""
+    import photonfdtd_b200 as pf
+    from photonfdtd_b200 import workloads as W
+    from photonfdtd_b200.batch import BatchTE, value_and_grad_eps
+    sizes = W.config4_sizes()
+    sims = [W.config4_instance(pf, nx, ny, i=k) for k, (nx, ny) in enumerate(sizes)]
+    wins = [W.design_window_box(nx, ny, 64) for nx, ny in sizes]
+    t0 = time.perf_counter()
+    b = BatchTE(sims, wins)
+    setup = time.perf_counter() - t0
+    eps = b.design_eps()
+    value_and_grad_eps(b, eps)  # warm-up: graph capture
+    l0 = b.info()["launches"]
+    times, fwd, adj = [], [], []
+    for _ in range(iters):
+        t0 = time.perf_counter()
+        vals, grad = value_and_grad_eps(b, eps)
+        times.append(time.perf_counter() - t0)
+        t1 = time.perf_counter()
+        F = b.forward()
+        t2 = time.perf_counter()
+        b.adjoint(2.0 * F)
+        t3 = time.perf_counter()
+        fwd.append(t2 - t1)
+        adj.append(t3 - t2)
+    info = b.info()
+    launches = (info["launches"] - l0) // (2 * iters)
+    cells = b.ncell * b.n_steps
+    out = {"metric": "adjoint grad s/iter (256-instance batch)", "value": round(min(times), 3),
+           "unit": "s/iter", "higher_is_better": False, "iters": iters,
+           "workload": ADJ_WORKLOAD, "cells": b.ncell, "steps": b.n_steps,
+           "forward_s": round(min(fwd), 3), "adjoint_s": round(min(adj), 3),
+           "forward_gcell_per_s": round(cells / min(fwd) / 1e9, 2),
+           "checkpoint_every": info["checkpoint_every"], "segments": info["segments"],
+           "setup_s": round(setup, 2), "gpu_launches_per_iter": int(launches),
+           "objective_sum": float(np.sum(vals)), "grad_max": float(np.max(np.abs(grad)))}
+    b.close()
+    if cpu:
+        out["cpu_baseline"] = adjoint_cpu_baseline(sims[0], wins[0], cells)
+    return out
+
+
+def adjoint_cpu_baseline(sim, win, cells_total, steps=60):
+    """The NumPy forward + adjoint restatement (oracle/adjoint2d.py) on the
+    first instance for `steps` steps, scaled by cell-steps to the batch."""
+    from oracle.adjoint2d import TEAdjointRun, objective_cotangent
+    run = TEAdjointRun(sim, win, n_steps=steps)
+    t0 = time.perf_counter()
+    F = run.forward()
+    run.adjoint(objective_cotangent(F))
+    wall = time.perf_counter() - t0
+    rate = run.nx * run.ny * steps / wall
+    return {"value": round(cells_total / rate, 1), "unit": "s/iter", "cores": 1, "kind": "port",
+            "sample": f"instance 0 ({run.nx}x{run.ny}), {steps} steps forward + adjoint in "
+                      f"{wall:.1f} s, scaled by cell-steps to the 256-instance, 4000-step batch"}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -324,6 +398,15 @@ def main():
                        "l2": "state ~6 GB > 126 MB L2: inputs larger than L2, no flush"},
             "roofline": roof, "e2e": e2e, "gpu_launches": int(sum(launches)),
             "clocks": clk.summary()}
+    if not args.no_adjoint:
+        adj = adjoint_bench(max(1, args.adjoint_iters), rank == 0 and world == 1 and
+                            not args.no_cpu_baseline)
+        if dist is not None:
+            tt = torch.tensor([adj["value"]], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            adj["value"] = round(float(tt.item()), 3)
+            adj["scaling"] = "weak (one batch per rank)"
+        line["adjoint"] = adj
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.size)
     if dist is not None:

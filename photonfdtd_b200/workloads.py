@@ -171,6 +171,11 @@ def config4_eps(nx: int, ny: int, rho: np.ndarray, dtype=np.float32) -> np.ndarr
     return eps.astype(dtype)
 
 
+def design_window_box(nx: int, ny: int, design: int) -> Tuple[int, int, int]:
+    """(i0, j0, n) of the centred design window."""
+    return nx // 2 - design // 2, ny // 2 - design // 2, design
+
+
 def design_window(nx: int, ny: int, design: int) -> Tuple[slice, slice]:
     i0, j0 = nx // 2 - design // 2, ny // 2 - design // 2
     return slice(i0, i0 + design), slice(j0, j0 + design)
