@@ -259,7 +259,8 @@ int pfb_set_dft(pf_batch *b, int n_freq, const double *phase);
 /* Lays out the pooled arrays and uploads everything. checkpoint_every = K:
  * the state is stored every K steps (ceil(n_steps/K) - 1 states), and the
  * adjoint replays K steps at a time; K >= n_steps stores no state and needs
- * no replay. tile_rows: x rows per 32-wide tile (8, 16 or 32; a thread
+ * no replay. K = 0 makes a forward-only batch: no adjoint state is allocated
+ * and pfb_adjoint / pfb_read_grad return PF_ERR_STATE. tile_rows: x rows per 32-wide tile (8, 16 or 32; a thread
  * updates tile_rows / 8 consecutive rows). */
 int pfb_finalize(pf_batch *b, int checkpoint_every, int tile_rows);
 
@@ -290,6 +291,57 @@ int pfb_info(const pf_batch *b, int64_t *out, int n_out);
 void *pfb_stream(pf_batch *b);
 const char *pfb_last_error(const pf_batch *b);
 void pfb_destroy(pf_batch *b);
+
+/* ------------------------------------------------------------------------
+ * Surrogate network kernels (pfs_*). The reference has no learned surrogate:
+ * these are the training and inference routines of this library's
+ * convolutional encoder-decoder (photonfdtd_b200/surrogate.py), which maps
+ * a design density to its transmission spectrum. All pointers are device
+ * pointers owned by the caller; BF16 buffers are passed as void*; `stream`
+ * is a cudaStream_t (NULL = default stream). Calls are asynchronous and
+ * allocate nothing. Error text: pfs_last_error() (per host thread).
+ * ---------------------------------------------------------------------- */
+const char *pfs_last_error(void);
+/* C (M x N, FP32, ld ldc) = alpha * A B^T + beta * C; A M x K and B N x K
+ * row-major BF16, K a multiple of 32, lda / ldb multiples of 8, A and B
+ * 16-byte aligned. Tensor cores (BF16 in, FP32 accumulate). */
+int pfs_gemm_bf16(int M, int N, int K, const void *A, int lda, const void *B, int ldb,
+                  float *C, int ldc, float alpha, float beta, void *stream);
+/* Lowering of a 2D convolution (kernel kh x kw, stride, zero padding ph
+ * rows / pw columns) over NHWC BF16 input x (nb, H, W, C): col rows
+ * (b, oy, ox), columns (ky * kw + kx) * C + c, zero-padded to Kp. */
+int pfs_im2col(int nb, int H, int W, int C, int kh, int kw, int stride, int ph, int pw,
+               const void *x, void *col, int Kp, void *stream);
+/* Adjoint of pfs_im2col: FP32 dcol -> FP32 dx (nb, H, W, C), overwritten. */
+int pfs_col2im(int nb, int H, int W, int C, int kh, int kw, int stride, int ph, int pw,
+               const float *dcol, int Kp, float *dx, void *stream);
+/* y = act(x + bias) on an M x N matrix (bias may be NULL; relu 0/1); FP32
+ * and / or BF16 outputs. */
+int pfs_bias_act(int64_t M, int N, const float *x, const float *bias, int relu, float *y32,
+                 void *y16, void *stream);
+/* Backward of pfs_bias_act: d = dy * (y > 0) (or dy) into d32 / d16 (either
+ * may be NULL) and dbias[n] = sum_m d (if dbias; part holds row_blocks * N
+ * floats of scratch, row_blocks in [1, 65535]). */
+int pfs_act_bwd(int64_t M, int N, const float *dy, const float *y, int relu, float *d32,
+                void *d16, float *dbias, float *part, int row_blocks, void *stream);
+/* out (Cc x ldo) = transpose of in (R x Cc, ld ldi), columns R..ldo-1 zero. */
+int pfs_transpose_bf16(int R, int Cc, const void *in, int ldi, void *out, int ldo,
+                       void *stream);
+int pfs_to_bf16(int64_t n, const float *x, void *y, void *stream);
+/* Nearest 2x upsampling along W of a (nb, W, C) BF16 tensor, and its adjoint
+ * (FP32, (nb, 2W, C) -> (nb, W, C)). */
+int pfs_upsample2(int64_t nb, int W, int C, const void *x, void *y, void *stream);
+int pfs_upsample2_bwd(int64_t nb, int W, int C, const float *dy, float *dx, void *stream);
+/* Mean squared error of the first `used` columns of y (rows x ld) against t
+ * (rows x used): grad (rows x ld) = 2 (y - t) / (rows * used) in those
+ * columns, 0 elsewhere, and nparts partial losses (their sum is the loss). */
+int pfs_mse(int64_t rows, int used, int ld, const float *y, const float *t, float *grad,
+            float *loss_parts, int nparts, void *stream);
+/* One Adam step (bias-corrected, step >= 1; decoupled weight decay:
+ * w -= lr * (m_hat / (sqrt(v_hat) + eps) + wd * w)) on FP32 master weights
+ * w, refreshing the BF16 copy w16 if given. */
+int pfs_adam(int64_t n, float *w, const float *g, float *m, float *v, float lr, float b1,
+             float b2, float eps, int step, float wd, void *w16, void *stream);
 
 #ifdef __cplusplus
 }

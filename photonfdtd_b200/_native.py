@@ -84,6 +84,22 @@ SIGNATURES = {
     "pfb_stream": (_vp, [_vp]),
     "pfb_last_error": (C.c_char_p, [_vp]),
     "pfb_destroy": (None, [_vp]),
+    # surrogate network kernels (device pointers as void*)
+    "pfs_last_error": (C.c_char_p, []),
+    "pfs_gemm_bf16": (C.c_int, [C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp,
+                                C.c_int, C.c_float, C.c_float, _vp]),
+    "pfs_im2col": (C.c_int, [C.c_int] * 9 + [_vp, _vp, C.c_int, _vp]),
+    "pfs_col2im": (C.c_int, [C.c_int] * 9 + [_vp, C.c_int, _vp, _vp]),
+    "pfs_bias_act": (C.c_int, [_i64, C.c_int, _vp, _vp, C.c_int, _vp, _vp, _vp]),
+    "pfs_act_bwd": (C.c_int, [_i64, C.c_int, _vp, _vp, C.c_int, _vp, _vp, _vp, _vp, C.c_int,
+                              _vp]),
+    "pfs_transpose_bf16": (C.c_int, [C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp]),
+    "pfs_to_bf16": (C.c_int, [_i64, _vp, _vp, _vp]),
+    "pfs_upsample2": (C.c_int, [_i64, C.c_int, C.c_int, _vp, _vp, _vp]),
+    "pfs_upsample2_bwd": (C.c_int, [_i64, C.c_int, C.c_int, _vp, _vp, _vp]),
+    "pfs_mse": (C.c_int, [_i64, C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp]),
+    "pfs_adam": (C.c_int, [_i64, _vp, _vp, _vp, _vp, C.c_float, C.c_float, C.c_float, C.c_float,
+                           C.c_int, C.c_float, _vp, _vp]),
 }
 
 

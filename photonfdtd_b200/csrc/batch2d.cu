@@ -62,6 +62,7 @@ struct pf_batch {
   bool merge_post = true;  // no E-source group sits on an output-line cell
   int n_h_groups = 0;      // source groups on Hz
   bool finalized = false, fwd_done = false, ring_last = false;
+  bool fwd_only = false;  // finalized with checkpoint_every = 0: no adjoint state
   bool fd[2] = {false, false};
   double rd[2] = {1, 1};
   std::vector<long long> s_cell;
@@ -170,7 +171,7 @@ BArgs<T> bargs(pf_batch* b) {
   a.base = b->base;
   a.ring = (T*)b->ring;
   a.n_design = b->n_design;
-  a.ring_len = b->ckpt;
+  a.ring_len = b->fwd_only ? 1 : b->ckpt;
   return a;
 }
 
@@ -353,7 +354,8 @@ int forward_t(pf_batch* b) {
   B_CUDA(b, cudaMemsetAsync(b->acc, 0, (size_t)b->nline * b->n_freq * 16, b->stream));
   const long long K = b->ckpt;
   for (long long s0 = 0; s0 < b->n_steps; s0 += K) {
-    if (s0 > 0 && (rc = state_copy(b, s0 / K - 1, true))) return rc;  // segment 0 starts at zero
+    if (s0 > 0 && !b->fwd_only && (rc = state_copy(b, s0 / K - 1, true)))
+      return rc;  // segment 0 starts at zero
     if ((rc = set_base(b, s0))) return rc;
     if ((rc = run_chunk<T>(b, 0, std::min(K, b->n_steps - s0)))) return rc;
   }
@@ -518,13 +520,15 @@ int pfb_set_dft(pf_batch* b, int n_freq, const double* phase) {
 int pfb_finalize(pf_batch* b, int checkpoint_every, int tile_rows) {
   if (!b) return PF_ERR_INVALID;
   if (b->finalized) return bfail(b, PF_ERR_STATE, "pfb_finalize called twice");
-  if (checkpoint_every < 1) return bfail(b, PF_ERR_INVALID, "checkpoint_every must be >= 1");
+  if (checkpoint_every < 0) return bfail(b, PF_ERR_INVALID, "checkpoint_every must be >= 0");
   if (tile_rows != 8 && tile_rows != 16 && tile_rows != 32)
     return bfail(b, PF_ERR_INVALID, "tile_rows must be 8, 16 or 32");
   if (b->n_freq < 1) return bfail(b, PF_ERR_STATE, "pfb_set_dft must come before pfb_finalize");
   for (int k = 0; k < b->n_inst; ++k)
     if (b->inst[k].nx == 0) return bfail(b, PF_ERR_STATE, "instance %d not set", k);
-  b->ckpt = (int)std::min<long long>(checkpoint_every, b->n_steps);
+  b->fwd_only = checkpoint_every == 0;
+  // forward-only batches run in graph chunks of at most 512 steps
+  b->ckpt = (int)std::min<long long>(b->fwd_only ? 512 : checkpoint_every, b->n_steps);
   b->rows = tile_rows / kWarps;
   const size_t S = b->rb;
   std::vector<int> mp[4];
@@ -607,22 +611,28 @@ int pfb_finalize(pf_batch* b, int checkpoint_every, int tile_rows) {
     if ((rc = bup(b, (void**)&b->maps[q], mp[q].data(), mp[q].size() * 4))) return rc;
   for (void** p : {&b->Ex, &b->Ey, &b->Hz})
     if ((rc = balloc(b, p, b->ncell * S))) return rc;
-  for (int q = 0; q < 3; ++q)
-    if ((rc = balloc(b, &b->aE[q], b->ncell * S))) return rc;
-  for (int q = 0; q < 4; ++q) {
+  for (int q = 0; q < 4; ++q)
     if ((rc = balloc(b, &b->psi[q], b->npsi[q] * S))) return rc;
-    if ((rc = balloc(b, &b->apsi[q], b->npsi[q] * S))) return rc;
-    if ((rc = balloc(b, &b->g[q], b->ncell * S))) return rc;
+  if (!b->fwd_only) {
+    for (int q = 0; q < 3; ++q)
+      if ((rc = balloc(b, &b->aE[q], b->ncell * S))) return rc;
+    for (int q = 0; q < 4; ++q) {
+      if ((rc = balloc(b, &b->apsi[q], b->npsi[q] * S))) return rc;
+      if ((rc = balloc(b, &b->g[q], b->ncell * S))) return rc;
+    }
+    if ((rc = balloc(b, (void**)&b->grad, b->n_design * 8))) return rc;
+    if ((rc = balloc(b, (void**)&b->cot, (size_t)b->nline * b->n_freq * 16))) return rc;
   }
-  if ((rc = balloc(b, (void**)&b->grad, b->n_design * 8))) return rc;
   if ((rc = balloc(b, &b->design_stage, b->n_design * S))) return rc;
-  if ((rc = balloc(b, &b->ring, (size_t)b->ckpt * b->n_design * 2 * S))) return rc;
+  const long long ring_slots = b->fwd_only ? 1 : b->ckpt;
+  if ((rc = balloc(b, &b->ring, (size_t)ring_slots * b->n_design * 2 * S))) return rc;
   b->state_elems = 3 * b->ncell + b->npsi[0] + b->npsi[1] + b->npsi[2] + b->npsi[3];
   const long long nseg = (b->n_steps + b->ckpt - 1) / b->ckpt;
   // checkpoints of segments 1 .. nseg-1 (segment 0 starts from the zero state)
-  if ((rc = balloc(b, &b->ckpt_buf, (size_t)(nseg - 1) * b->state_elems * S))) return rc;
+  if (!b->fwd_only &&
+      (rc = balloc(b, &b->ckpt_buf, (size_t)(nseg - 1) * b->state_elems * S)))
+    return rc;
   if ((rc = balloc(b, (void**)&b->acc, (size_t)b->nline * b->n_freq * 16))) return rc;
-  if ((rc = balloc(b, (void**)&b->cot, (size_t)b->nline * b->n_freq * 16))) return rc;
   if ((rc = bup(b, (void**)&b->lcell, lcell.data(), lcell.size() * 8))) return rc;
   if ((rc = bup(b, (void**)&b->phase, b->h_phase.data(), b->h_phase.size() * 8))) return rc;
   if ((rc = balloc(b, (void**)&b->base, 8))) return rc;
@@ -694,6 +704,7 @@ int pfb_forward(pf_batch* b) {
 
 int pfb_adjoint(pf_batch* b, const double* cotangent) {
   if (!b) return PF_ERR_INVALID;
+  if (b->fwd_only) return bfail(b, PF_ERR_STATE, "forward-only batch (checkpoint_every = 0)");
   if (!b->fwd_done)
     return bfail(b, PF_ERR_STATE, "pfb_adjoint needs a pfb_forward of the current design");
   if (!cotangent) return bfail(b, PF_ERR_INVALID, "cotangent is NULL");
@@ -714,6 +725,7 @@ int pfb_read_dft(pf_batch* b, double* dst) {
 int pfb_read_grad(pf_batch* b, double* dst) {
   if (!b) return PF_ERR_INVALID;
   if (!b->finalized || !dst) return bfail(b, PF_ERR_INVALID, "bad pfb_read_grad");
+  if (b->fwd_only) return bfail(b, PF_ERR_STATE, "forward-only batch (checkpoint_every = 0)");
   B_CUDA(b, cudaMemcpyAsync(dst, b->grad, (size_t)b->n_design * 8, cudaMemcpyDeviceToHost,
                             b->stream));
   B_CUDA(b, cudaStreamSynchronize(b->stream));

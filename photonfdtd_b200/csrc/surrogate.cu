@@ -1,0 +1,467 @@
+// surrogate.cu - training and inference kernels of the learned surrogate
+// (a convolutional encoder-decoder mapping a design density to its complex
+// transmission spectrum).
+//
+// Every layer of the network is expressed with these few device routines,
+// all hand-written here:
+//   * pfs_gemm_bf16: C = alpha * A B^T + beta * C, A (M x K) and B (N x K)
+//     row-major BF16 (K contiguous), C row-major FP32. Tensor cores through
+//     mma.sync m16n8k16 (BF16 inputs, FP32 accumulate); 64 x 64 x 32 block
+//     tiles, 4 warps of 32 x 32, operands staged in padded shared memory with
+//     a register prefetch of the next K slice.
+//   * im2col (BF16, K padded with zeros to a multiple of 32) and its adjoint
+//     col2im (FP32, a gather over the kernel taps: deterministic);
+//   * bias + ReLU with FP32 and BF16 outputs, and its backward with a
+//     deterministic column reduction for the bias gradient;
+//   * BF16 transposes, FP32 -> BF16 conversion, nearest 2x upsampling along
+//     the width and its adjoint, the mean-squared-error loss gradient and an
+//     Adam step on FP32 master weights that refreshes their BF16 copies.
+// Activations are NHWC. Nothing here allocates: the caller owns every buffer
+// and passes its stream (NULL = the default stream).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/pfb200.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int sfail(int code, const char* msg) {
+  g_err = msg;
+  return code;
+}
+
+int cuda_status(const char* what) {
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) return PF_OK;
+  char buf[256];
+  snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+  g_err = buf;
+  return PF_ERR_CUDA;
+}
+
+// ---- GEMM ------------------------------------------------------------------
+constexpr int BM = 64, BN = 64, BK = 32, PADK = BK + 8;  // padded rows: fewer bank conflicts
+
+__device__ __forceinline__ void mma_bf16(float c[4], const uint32_t a[4], const uint32_t b[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+      "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// One 16-byte chunk (8 BF16) of row r, columns k0..k0+7 of a row-major
+// matrix with `rows` rows and leading dimension ld, or zeros out of range.
+__device__ __forceinline__ uint4 ld_chunk(const __nv_bfloat16* p, int rows, int ld, int r, int k0) {
+  if (r >= rows) return make_uint4(0, 0, 0, 0);
+  return *reinterpret_cast<const uint4*>(p + (long long)r * ld + k0);
+}
+
+// C[M x N] = alpha * sum_k A[m][k] B[n][k] + beta * C. K % 32 == 0; lda, ldb
+// multiples of 8 (16-byte rows); pointers 16-byte aligned.
+__global__ void __launch_bounds__(128) k_gemm_bf16(int M, int N, int K, const __nv_bfloat16* A,
+                                                   int lda, const __nv_bfloat16* B, int ldb,
+                                                   float* C, int ldc, float alpha, float beta) {
+  __shared__ __align__(16) __nv_bfloat16 As[BM][PADK];
+  __shared__ __align__(16) __nv_bfloat16 Bs[BN][PADK];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  const int g = lane >> 2, tg = lane & 3;
+  float acc[2][4][4];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.f;
+  // each thread stages two 16-byte chunks of A and two of B per K slice:
+  // chunk q = tid + 128 * h -> row q / 4, columns (q % 4) * 8
+  uint4 ra[2], rb[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int q = tid + 128 * h, r = q >> 2, kc = (q & 3) * 8;
+    ra[h] = ld_chunk(A, M, lda, m0 + r, kc);
+    rb[h] = ld_chunk(B, N, ldb, n0 + r, kc);
+  }
+  for (int k0 = 0; k0 < K; k0 += BK) {
+    __syncthreads();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int q = tid + 128 * h, r = q >> 2, kc = (q & 3) * 8;
+      *reinterpret_cast<uint4*>(&As[r][kc]) = ra[h];
+      *reinterpret_cast<uint4*>(&Bs[r][kc]) = rb[h];
+    }
+    __syncthreads();
+    if (k0 + BK < K) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int q = tid + 128 * h, r = q >> 2, kc = (q & 3) * 8;
+        ra[h] = ld_chunk(A, M, lda, m0 + r, k0 + BK + kc);
+        rb[h] = ld_chunk(B, N, ldb, n0 + r, k0 + BK + kc);
+      }
+    }
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 16) {
+      uint32_t af[2][4], bf[4][2];
+#pragma unroll
+      for (int a = 0; a < 2; ++a) {
+        const int r = wm + a * 16 + g;
+        af[a][0] = *reinterpret_cast<const uint32_t*>(&As[r][kk + tg * 2]);
+        af[a][1] = *reinterpret_cast<const uint32_t*>(&As[r + 8][kk + tg * 2]);
+        af[a][2] = *reinterpret_cast<const uint32_t*>(&As[r][kk + tg * 2 + 8]);
+        af[a][3] = *reinterpret_cast<const uint32_t*>(&As[r + 8][kk + tg * 2 + 8]);
+      }
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const int n = wn + b * 8 + g;
+        bf[b][0] = *reinterpret_cast<const uint32_t*>(&Bs[n][kk + tg * 2]);
+        bf[b][1] = *reinterpret_cast<const uint32_t*>(&Bs[n][kk + tg * 2 + 8]);
+      }
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) mma_bf16(acc[a][b], af[a], bf[b]);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int r = m0 + wm + a * 16 + g + (c >= 2 ? 8 : 0);
+        const int n = n0 + wn + b * 8 + tg * 2 + (c & 1);
+        if (r < M && n < N) {
+          float* o = C + (long long)r * ldc + n;
+          const float v = alpha * acc[a][b][c];
+          *o = beta == 0.f ? v : v + beta * *o;
+        }
+      }
+}
+
+// ---- convolution lowering ----------------------------------------------------
+// col[(b, oy, ox)][k], k = (ky * kw + kx) * C + c for k < kh*kw*C, zero above.
+__global__ void k_im2col(int nb, int H, int W, int C, int kh, int kw, int stride, int ph, int pw,
+                         int Ho, int Wo, const __nv_bfloat16* x, __nv_bfloat16* col, int Kp) {
+  const long long total = (long long)nb * Ho * Wo * Kp;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(t % Kp);
+    const long long m = t / Kp;
+    __nv_bfloat16 v = __float2bfloat16(0.f);
+    if (k < kh * kw * C) {
+      const int c = k % C, tap = k / C, kx = tap % kw, ky = tap / kw;
+      const int ox = (int)(m % Wo), oy = (int)((m / Wo) % Ho), b = (int)(m / ((long long)Wo * Ho));
+      const int iy = oy * stride - ph + ky, ix = ox * stride - pw + kx;
+      if (iy >= 0 && iy < H && ix >= 0 && ix < W) v = x[(((long long)b * H + iy) * W + ix) * C + c];
+    }
+    col[t] = v;
+  }
+}
+
+// dx[b, iy, ix, c] = sum over the taps (ky, kx) whose output position
+// (oy, ox) = ((iy + ph - ky) / stride, (ix + pw - kx) / stride) is integral
+// and in range of dcol[(b, oy, ox)][(ky * kw + kx) * C + c].
+__global__ void k_col2im(int nb, int H, int W, int C, int kh, int kw, int stride, int ph, int pw,
+                         int Ho, int Wo, const float* dcol, int Kp, float* dx) {
+  const long long total = (long long)nb * H * W * C;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t % C);
+    const int ix = (int)((t / C) % W), iy = (int)((t / ((long long)C * W)) % H);
+    const int b = (int)(t / ((long long)C * W * H));
+    float s = 0.f;
+    for (int ky = 0; ky < kh; ++ky) {
+      const int ny = iy + ph - ky;
+      if (ny < 0 || ny % stride) continue;
+      const int oy = ny / stride;
+      if (oy >= Ho) continue;
+      for (int kx = 0; kx < kw; ++kx) {
+        const int nx = ix + pw - kx;
+        if (nx < 0 || nx % stride) continue;
+        const int ox = nx / stride;
+        if (ox >= Wo) continue;
+        s += dcol[(((long long)b * Ho + oy) * Wo + ox) * Kp + (ky * kw + kx) * C + c];
+      }
+    }
+    dx[t] = s;
+  }
+}
+
+// y = act(x + bias) over an M x N row-major matrix; FP32 and BF16 outputs
+// (either may be NULL).
+__global__ void k_bias_act(long long M, int N, const float* x, const float* bias, int relu,
+                           float* y32, __nv_bfloat16* y16) {
+  const long long total = M * N;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    float v = x[t] + (bias ? bias[t % N] : 0.f);
+    if (relu) v = fmaxf(v, 0.f);
+    if (y32) y32[t] = v;
+    if (y16) y16[t] = __float2bfloat16(v);
+  }
+}
+
+// dpre = dy * (y > 0) (or dy), stored FP32 and BF16, and per row block the
+// column sums of dpre: part[blockIdx.y][n]. Blocks of 32 columns x 8 row
+// lanes; each row block strides the rows, then a fixed-order reduction.
+__global__ void k_act_bwd(long long M, int N, const float* dy, const float* y, int relu,
+                          float* d32, __nv_bfloat16* d16, float* part) {
+  __shared__ float sh[8][33];
+  const int n = blockIdx.x * 32 + threadIdx.x;
+  float s = 0.f;
+  for (long long m = (long long)blockIdx.y * 8 + threadIdx.y; m < M; m += (long long)gridDim.y * 8) {
+    if (n < N) {
+      const long long t = m * N + n;
+      float v = dy[t];
+      if (relu && !(y[t] > 0.f)) v = 0.f;
+      if (d32) d32[t] = v;
+      if (d16) d16[t] = __float2bfloat16(v);
+      s += v;
+    }
+  }
+  sh[threadIdx.y][threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.y == 0 && n < N && part) {
+    float r = 0.f;
+    for (int q = 0; q < 8; ++q) r += sh[q][threadIdx.x];
+    part[(long long)blockIdx.y * N + n] = r;
+  }
+}
+
+// dbias[n] = sum over row blocks of part[q][n], in order.
+__global__ void k_colsum(int R, int N, const float* part, float* out) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  float r = 0.f;
+  for (int q = 0; q < R; ++q) r += part[(long long)q * N + n];
+  out[n] = r;
+}
+
+// out[c][r] = in[r][c] for an R x Cc row-major BF16 matrix; out has leading
+// dimension ldo (>= R, extra columns zero-filled up to ldo).
+__global__ void k_transpose_bf16(int R, int Cc, const __nv_bfloat16* in, int ldi,
+                                 __nv_bfloat16* out, int ldo) {
+  __shared__ __nv_bfloat16 tile[32][33];
+  const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+  for (int q = threadIdx.y; q < 32; q += blockDim.y) {
+    const int r = r0 + q, c = c0 + threadIdx.x;
+    tile[q][threadIdx.x] = (r < R && c < Cc) ? in[(long long)r * ldi + c] : __float2bfloat16(0.f);
+  }
+  __syncthreads();
+  for (int q = threadIdx.y; q < 32; q += blockDim.y) {
+    const int c = c0 + q, r = r0 + threadIdx.x;
+    if (c < Cc && r < ldo) out[(long long)c * ldo + r] = tile[threadIdx.x][q];
+  }
+}
+
+__global__ void k_to_bf16(long long n, const float* x, __nv_bfloat16* y) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x)
+    y[t] = __float2bfloat16(x[t]);
+}
+
+// Nearest 2x upsampling along the width of an (nb, W, C) tensor (H = 1):
+// y[b, 2w + s, c] = x[b, w, c]; the backward sums the two copies.
+__global__ void k_upsample2(long long nb, int W, int C, const __nv_bfloat16* x, __nv_bfloat16* y) {
+  const long long total = nb * 2 * W * C;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t % C);
+    const long long w2 = (t / C) % (2 * W), b = t / ((long long)C * 2 * W);
+    y[t] = x[(b * W + w2 / 2) * C + c];
+  }
+}
+
+__global__ void k_upsample2_bwd(long long nb, int W, int C, const float* dy, float* dx) {
+  const long long total = nb * W * C;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t % C);
+    const long long w = (t / C) % W, b = t / ((long long)C * W);
+    const long long o = (b * 2 * W + 2 * w) * C + c;
+    dx[t] = dy[o] + dy[o + C];
+  }
+}
+
+// MSE of the first `used` columns of y (rows x ld, FP32) against compact t
+// (rows x used): grad (rows x ld) = 2 (y - t) / (rows * used) there, zero in
+// the other columns; per-block partial losses in fixed order.
+__global__ void k_mse(long long rows, int used, int ld, const float* y, const float* t,
+                      float* grad, float* loss) {
+  __shared__ float sh[256];
+  const long long n = rows * ld;
+  const float inv = 1.f / (float)(rows * used);
+  float s = 0.f;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(q % ld);
+    if (c < used) {
+      const float d = y[q] - t[(q / ld) * used + c];
+      grad[q] = 2.f * d * inv;
+      s += d * d;
+    } else {
+      grad[q] = 0.f;
+    }
+  }
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) loss[blockIdx.x] = sh[0] * inv;
+}
+
+// Adam on FP32 master weights (bias-corrected, weight decay decoupled from
+// the gradient statistics), then the BF16 copy.
+__global__ void k_adam(long long n, float* w, const float* g, float* m, float* v, float lr,
+                       float b1, float b2, float eps, float c1, float c2, float wd,
+                       __nv_bfloat16* w16) {
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const float gt = g[t];
+    const float mt = b1 * m[t] + (1.f - b1) * gt;
+    const float vt = b2 * v[t] + (1.f - b2) * gt * gt;
+    m[t] = mt;
+    v[t] = vt;
+    const float wn = w[t] - lr * ((mt / c1) / (sqrtf(vt / c2) + eps) + wd * w[t]);
+    w[t] = wn;
+    if (w16) w16[t] = __float2bfloat16(wn);
+  }
+}
+
+unsigned grid_for(long long n, int block) {
+  long long g = (n + block - 1) / block;
+  if (g > 148LL * 32) g = 148LL * 32;
+  return (unsigned)(g < 1 ? 1 : g);
+}
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+
+}  // namespace
+
+extern "C" {
+
+const char* pfs_last_error(void) { return g_err.c_str(); }
+
+int pfs_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C,
+                  int ldc, float alpha, float beta, void* stream) {
+  if (M < 0 || N < 0 || K < 0 || (M && N && (!A || !B || !C)))
+    return sfail(PF_ERR_INVALID, "pfs_gemm_bf16: bad sizes or NULL operand");
+  if (K % 32 || lda % 8 || ldb % 8 || lda < K || ldb < K || ldc < N)
+    return sfail(PF_ERR_INVALID,
+                 "pfs_gemm_bf16: K must be a multiple of 32, lda/ldb multiples of 8 and >= K");
+  if (!aligned16(A) || !aligned16(B))
+    return sfail(PF_ERR_INVALID, "pfs_gemm_bf16: A and B must be 16-byte aligned");
+  if (!M || !N) return PF_OK;
+  if (K == 0) {
+    return sfail(PF_ERR_INVALID, "pfs_gemm_bf16: K must be positive");
+  }
+  const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+  if (grid.y > 65535) return sfail(PF_ERR_INVALID, "pfs_gemm_bf16: M too large");
+  k_gemm_bf16<<<grid, 128, 0, (cudaStream_t)stream>>>(
+      M, N, K, (const __nv_bfloat16*)A, lda, (const __nv_bfloat16*)B, ldb, C, ldc, alpha, beta);
+  return cuda_status("pfs_gemm_bf16");
+}
+
+int pfs_im2col(int nb, int H, int W, int C, int kh, int kw, int stride, int ph, int pw,
+               const void* x, void* col, int Kp, void* stream) {
+  if (nb < 1 || H < 1 || W < 1 || C < 1 || kh < 1 || kw < 1 || stride < 1 || ph < 0 || pw < 0 ||
+      !x || !col || Kp < kh * kw * C)
+    return sfail(PF_ERR_INVALID, "pfs_im2col: bad arguments");
+  const int Ho = (H + 2 * ph - kh) / stride + 1, Wo = (W + 2 * pw - kw) / stride + 1;
+  if (Ho < 1 || Wo < 1) return sfail(PF_ERR_INVALID, "pfs_im2col: empty output");
+  const long long n = (long long)nb * Ho * Wo * Kp;
+  k_im2col<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(
+      nb, H, W, C, kh, kw, stride, ph, pw, Ho, Wo, (const __nv_bfloat16*)x, (__nv_bfloat16*)col,
+      Kp);
+  return cuda_status("pfs_im2col");
+}
+
+int pfs_col2im(int nb, int H, int W, int C, int kh, int kw, int stride, int ph, int pw,
+               const float* dcol, int Kp, float* dx, void* stream) {
+  if (nb < 1 || H < 1 || W < 1 || C < 1 || kh < 1 || kw < 1 || stride < 1 || ph < 0 || pw < 0 ||
+      !dcol || !dx || Kp < kh * kw * C)
+    return sfail(PF_ERR_INVALID, "pfs_col2im: bad arguments");
+  const int Ho = (H + 2 * ph - kh) / stride + 1, Wo = (W + 2 * pw - kw) / stride + 1;
+  if (Ho < 1 || Wo < 1) return sfail(PF_ERR_INVALID, "pfs_col2im: empty output");
+  const long long n = (long long)nb * H * W * C;
+  k_col2im<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(nb, H, W, C, kh, kw, stride, ph,
+                                                               pw, Ho, Wo, dcol, Kp, dx);
+  return cuda_status("pfs_col2im");
+}
+
+int pfs_bias_act(int64_t M, int N, const float* x, const float* bias, int relu, float* y32,
+                 void* y16, void* stream) {
+  if (M < 0 || N < 1 || !x || (!y32 && !y16)) return sfail(PF_ERR_INVALID, "pfs_bias_act: bad arguments");
+  k_bias_act<<<grid_for(M * N, 256), 256, 0, (cudaStream_t)stream>>>(M, N, x, bias, relu, y32,
+                                                                     (__nv_bfloat16*)y16);
+  return cuda_status("pfs_bias_act");
+}
+
+int pfs_act_bwd(int64_t M, int N, const float* dy, const float* y, int relu, float* d32, void* d16,
+                float* dbias, float* part, int row_blocks, void* stream) {
+  if (M < 1 || N < 1 || !dy || (relu && !y) || row_blocks < 1 || row_blocks > 65535 ||
+      (dbias && !part))
+    return sfail(PF_ERR_INVALID, "pfs_act_bwd: bad arguments");
+  k_act_bwd<<<dim3((N + 31) / 32, row_blocks), dim3(32, 8), 0, (cudaStream_t)stream>>>(
+      M, N, dy, y, relu, d32, (__nv_bfloat16*)d16, dbias ? part : nullptr);
+  if (dbias) k_colsum<<<(N + 127) / 128, 128, 0, (cudaStream_t)stream>>>(row_blocks, N, part, dbias);
+  return cuda_status("pfs_act_bwd");
+}
+
+int pfs_transpose_bf16(int R, int Cc, const void* in, int ldi, void* out, int ldo, void* stream) {
+  if (R < 1 || Cc < 1 || !in || !out || ldi < Cc || ldo < R)
+    return sfail(PF_ERR_INVALID, "pfs_transpose_bf16: bad arguments");
+  const int rows = (ldo + 31) / 32;  // cover the zero fill up to ldo
+  k_transpose_bf16<<<dim3((Cc + 31) / 32, rows), dim3(32, 8), 0, (cudaStream_t)stream>>>(
+      R, Cc, (const __nv_bfloat16*)in, ldi, (__nv_bfloat16*)out, ldo);
+  return cuda_status("pfs_transpose_bf16");
+}
+
+int pfs_to_bf16(int64_t n, const float* x, void* y, void* stream) {
+  if (n < 0 || (n && (!x || !y))) return sfail(PF_ERR_INVALID, "pfs_to_bf16: bad arguments");
+  if (!n) return PF_OK;
+  k_to_bf16<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(n, x, (__nv_bfloat16*)y);
+  return cuda_status("pfs_to_bf16");
+}
+
+int pfs_upsample2(int64_t nb, int W, int C, const void* x, void* y, void* stream) {
+  if (nb < 1 || W < 1 || C < 1 || !x || !y) return sfail(PF_ERR_INVALID, "pfs_upsample2: bad arguments");
+  k_upsample2<<<grid_for(nb * 2 * W * C, 256), 256, 0, (cudaStream_t)stream>>>(
+      nb, W, C, (const __nv_bfloat16*)x, (__nv_bfloat16*)y);
+  return cuda_status("pfs_upsample2");
+}
+
+int pfs_upsample2_bwd(int64_t nb, int W, int C, const float* dy, float* dx, void* stream) {
+  if (nb < 1 || W < 1 || C < 1 || !dy || !dx) return sfail(PF_ERR_INVALID, "pfs_upsample2_bwd: bad arguments");
+  k_upsample2_bwd<<<grid_for(nb * W * C, 256), 256, 0, (cudaStream_t)stream>>>(nb, W, C, dy, dx);
+  return cuda_status("pfs_upsample2_bwd");
+}
+
+int pfs_mse(int64_t rows, int used, int ld, const float* y, const float* t, float* grad,
+            float* loss_parts, int nparts, void* stream) {
+  if (rows < 1 || used < 1 || ld < used || !y || !t || !grad || !loss_parts || nparts < 1)
+    return sfail(PF_ERR_INVALID, "pfs_mse: bad arguments");
+  k_mse<<<nparts, 256, 0, (cudaStream_t)stream>>>(rows, used, ld, y, t, grad, loss_parts);
+  return cuda_status("pfs_mse");
+}
+
+int pfs_adam(int64_t n, float* w, const float* g, float* m, float* v, float lr, float b1, float b2,
+             float eps, int step, float wd, void* w16, void* stream) {
+  if (n < 1 || !w || !g || !m || !v || step < 1) return sfail(PF_ERR_INVALID, "pfs_adam: bad arguments");
+  const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+  k_adam<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(n, w, g, m, v, lr, b1, b2, eps, c1,
+                                                             c2, wd, (__nv_bfloat16*)w16);
+  return cuda_status("pfs_adam");
+}
+
+}  // extern "C"

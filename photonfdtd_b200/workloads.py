@@ -183,9 +183,10 @@ def design_window(nx: int, ny: int, design: int) -> Tuple[slice, slice]:
 
 def config4_instance(pf, nx: int, ny: int, rho: np.ndarray = None, i: int = 0,
                      n_steps: int = 4000, n_freqs: int = 8, precision: str = "float32",
-                     design: int = 64):
+                     design: int = 64, band: Tuple[float, float] = (1.5e-6, 1.6e-6)):
     """One 2D TE instance: Ey line source at x index 20 over the interior, Ey
-    DFT on the output line at x index nx - 21, custom eps from the density."""
+    DFT on the output line at x index nx - 21 at n_freqs wavelengths evenly
+    spaced over `band`, custom eps from the density."""
     d = 20e-9
     pml = 12
     grid = pf.Grid(size=(nx * d, ny * d), cell_size=(d, d), pml_layers=(pml, pml, 0))
@@ -194,7 +195,7 @@ def config4_instance(pf, nx: int, ny: int, rho: np.ndarray = None, i: int = 0,
     ys = grid.coords[1]
     srcs = [pf.PointDipole(position=(float(xs[20]), float(ys[j])), component="Ey",
                            waveform=pulse) for j in range(pml, ny - pml)]
-    freqs = C_0 / np.linspace(1.5e-6, 1.6e-6, n_freqs)
+    freqs = C_0 / np.linspace(band[0], band[1], n_freqs)
     mon = pf.DFTMonitor(name="out", components=("Ey",), freqs=freqs,
                         plane_axis="x", plane_position=float(xs[nx - 21]))
     dt = _dt(d, 2)
@@ -205,3 +206,23 @@ def config4_instance(pf, nx: int, ny: int, rho: np.ndarray = None, i: int = 0,
     npdt = np.float32 if precision == "float32" else np.float64
     sim.eps_r = config4_eps(nx, ny, rho, dtype=npdt)
     return sim
+
+
+# --------------------------------------------------------------------------- #
+# config 5: the surrogate's design problem
+# --------------------------------------------------------------------------- #
+CONFIG5_SHAPE = (400, 250)
+CONFIG5_BAND = (1.4e-6, 1.7e-6)
+CONFIG5_FREQS = 32
+
+
+def config5_instance(pf, rho: np.ndarray = None, n_steps: int = 4000,
+                     precision: str = "float32"):
+    """The fixed config-4-style geometry of the surrogate problem: 400 x 250
+    cells, centred 64 x 64 design window, Ey DFT at 32 wavelengths evenly
+    spaced over 1.4-1.7 um. rho = None is the empty design (cladding only)."""
+    nx, ny = CONFIG5_SHAPE
+    if rho is None:
+        rho = np.zeros((64, 64))
+    return config4_instance(pf, nx, ny, rho=rho, n_steps=n_steps, n_freqs=CONFIG5_FREQS,
+                            precision=precision, design=64, band=CONFIG5_BAND)

@@ -1,0 +1,214 @@
+"""Surrogate kernels on the GPU against NumPy: the BF16 tensor-core GEMM at
+FP32-accumulation accuracy, the convolution lowering and its adjoint, the
+elementwise / reduction kernels, Adam, and the whole network's forward and
+reverse pass against the NumPy oracle (oracle/surrogate_ref.py) run with the
+same BF16 rounding of GEMM operands. A short training run must cut the loss."""
+import numpy as np
+import pytest
+
+from photonfdtd_b200 import _native as N
+from photonfdtd_b200.surrogate import SurrogateNet, init_params, plan
+from oracle.surrogate_ref import RefNet, bf16, col2im, im2col
+
+pytestmark = pytest.mark.gpu
+
+
+def _t():
+    import torch
+    return torch
+
+
+def _p(x):
+    return x.data_ptr()
+
+
+def _chk(rc):
+    assert rc == N.PF_OK, N.lib().pfs_last_error().decode()
+
+
+def _s():
+    return _t().cuda.current_stream().cuda_stream
+
+
+@pytest.mark.parametrize("M,Nn,K,beta", [(100, 70, 96, 0.0), (257, 33, 32, 0.5),
+                                          (64, 512, 2048, 0.0), (4096, 32, 32, 1.0)])
+def test_gemm_bf16(M, Nn, K, beta):
+    t = _t()
+    rng = np.random.default_rng(M + Nn + K)
+    A = bf16(rng.standard_normal((M, K)))
+    B = bf16(rng.standard_normal((Nn, K)))
+    C0 = rng.standard_normal((M, Nn))
+    dA = t.from_numpy(A.astype(np.float32)).cuda().to(t.bfloat16)
+    dB = t.from_numpy(B.astype(np.float32)).cuda().to(t.bfloat16)
+    dC = t.from_numpy(C0.astype(np.float32)).cuda()
+    _chk(N.lib().pfs_gemm_bf16(M, Nn, K, _p(dA), K, _p(dB), K, _p(dC), Nn, 1.5, beta, _s()))
+    got = dC.cpu().numpy().astype(np.float64)
+    want = 1.5 * A @ B.T + beta * C0.astype(np.float32)
+    assert np.max(np.abs(got - want)) <= 1e-5 * np.max(np.abs(want)) * np.sqrt(K)
+
+
+def test_gemm_rejects_bad_shapes():
+    L = N.lib()
+    assert L.pfs_gemm_bf16(4, 4, 20, 16, 20, 16, 20, 16, 4, 1.0, 0.0, None) == N.PF_ERR_INVALID
+    assert "multiple of 32" in L.pfs_last_error().decode()
+
+
+@pytest.mark.parametrize("shape,k,s,p", [((2, 9, 7, 3), (3, 3), 2, (1, 1)),
+                                         ((2, 1, 8, 64), (1, 3), 1, (0, 1)),
+                                         ((3, 16, 16, 5), (3, 3), 1, (1, 1))])
+def test_im2col_and_col2im(shape, k, s, p):
+    t = _t()
+    rng = np.random.default_rng(1)
+    x = bf16(rng.standard_normal(shape))
+    col, Ho, Wo = im2col(x, k[0], k[1], s, p[0], p[1])
+    Kp = (col.shape[1] + 31) // 32 * 32
+    dx = t.from_numpy(x.astype(np.float32)).cuda().to(t.bfloat16)
+    dcol = t.zeros((col.shape[0], Kp), dtype=t.bfloat16, device="cuda")
+    L = N.lib()
+    _chk(L.pfs_im2col(shape[0], shape[1], shape[2], shape[3], k[0], k[1], s, p[0], p[1], _p(dx),
+                      _p(dcol), Kp, _s()))
+    got = dcol.float().cpu().numpy()
+    assert np.array_equal(got[:, :col.shape[1]], col.astype(np.float32))
+    assert not got[:, col.shape[1]:].any()
+    g = rng.standard_normal((col.shape[0], Kp))
+    gd = t.from_numpy(g.astype(np.float32)).cuda()
+    out = t.empty(shape, dtype=t.float32, device="cuda")
+    _chk(L.pfs_col2im(shape[0], shape[1], shape[2], shape[3], k[0], k[1], s, p[0], p[1], _p(gd),
+                      Kp, _p(out), _s()))
+    want = col2im(g[:, :col.shape[1]].astype(np.float32).astype(np.float64), shape, k[0], k[1], s,
+                  p[0], p[1])
+    assert np.allclose(out.cpu().numpy(), want, rtol=1e-5, atol=1e-5)
+
+
+def test_elementwise_kernels():
+    t = _t()
+    L = N.lib()
+    rng = np.random.default_rng(2)
+    M, Nn = 1000, 96
+    x = rng.standard_normal((M, Nn)).astype(np.float32)
+    b = rng.standard_normal(Nn).astype(np.float32)
+    dx, db = t.from_numpy(x).cuda(), t.from_numpy(b).cuda()
+    y32 = t.empty_like(dx)
+    y16 = t.empty((M, Nn), dtype=t.bfloat16, device="cuda")
+    _chk(L.pfs_bias_act(M, Nn, _p(dx), _p(db), 1, _p(y32), _p(y16), _s()))
+    want = np.maximum(x + b, 0)
+    assert np.array_equal(y32.cpu().numpy(), want)
+    assert np.array_equal(y16.float().cpu().numpy(), bf16(want).astype(np.float32))
+    dy = rng.standard_normal((M, Nn)).astype(np.float32)
+    ddy = t.from_numpy(dy).cuda()
+    d16 = t.empty((M, Nn), dtype=t.bfloat16, device="cuda")
+    d32 = t.empty_like(ddy)
+    gb = t.empty(Nn, dtype=t.float32, device="cuda")
+    part = t.empty((7, Nn), dtype=t.float32, device="cuda")
+    _chk(L.pfs_act_bwd(M, Nn, _p(ddy), _p(y32), 1, _p(d32), _p(d16), _p(gb), _p(part), 7, _s()))
+    dpre = dy * (want > 0)
+    assert np.array_equal(d32.cpu().numpy(), dpre)
+    assert np.allclose(gb.cpu().numpy(), dpre.sum(axis=0), rtol=1e-5, atol=1e-4)
+    # transpose with zero fill
+    out = t.empty((Nn, 1008), dtype=t.bfloat16, device="cuda")
+    _chk(L.pfs_transpose_bf16(M, Nn, _p(d16), Nn, _p(out), 1008, _s()))
+    o = out.float().cpu().numpy()
+    assert np.array_equal(o[:, :M], d16.float().cpu().numpy().T) and not o[:, M:].any()
+    # upsample and its adjoint
+    u = t.from_numpy(x[:64].reshape(4, 16, 96)).cuda().to(t.bfloat16)
+    uo = t.empty((4, 32, 96), dtype=t.bfloat16, device="cuda")
+    _chk(L.pfs_upsample2(4, 16, 96, _p(u), _p(uo), _s()))
+    assert np.array_equal(uo.float().cpu().numpy(), np.repeat(u.float().cpu().numpy(), 2, axis=1))
+    g = t.from_numpy(rng.standard_normal((4, 32, 96)).astype(np.float32)).cuda()
+    gi = t.empty((4, 16, 96), dtype=t.float32, device="cuda")
+    _chk(L.pfs_upsample2_bwd(4, 16, 96, _p(g), _p(gi), _s()))
+    assert np.allclose(gi.cpu().numpy(), g.cpu().numpy().reshape(4, 16, 2, 96).sum(axis=2))
+    # MSE over the first 2 of 32 columns
+    yy = t.from_numpy(rng.standard_normal((50, 32)).astype(np.float32)).cuda()
+    tt = t.from_numpy(rng.standard_normal((50, 2)).astype(np.float32)).cuda()
+    gr = t.empty_like(yy)
+    lp = t.empty(16, dtype=t.float32, device="cuda")
+    _chk(L.pfs_mse(50, 2, 32, _p(yy), _p(tt), _p(gr), _p(lp), 16, _s()))
+    d = yy.cpu().numpy()[:, :2] - tt.cpu().numpy()
+    assert np.isclose(lp.sum().item(), np.mean(d ** 2), rtol=1e-5)
+    assert np.allclose(gr.cpu().numpy()[:, :2], 2 * d / 100, rtol=1e-5)
+    assert not gr.cpu().numpy()[:, 2:].any()
+
+
+def test_adam_step():
+    t = _t()
+    rng = np.random.default_rng(3)
+    w = rng.standard_normal(1000).astype(np.float32)
+    g = rng.standard_normal(1000).astype(np.float32)
+    dw, dg = t.from_numpy(w.copy()).cuda(), t.from_numpy(g).cuda()
+    m, v = t.zeros_like(dw), t.zeros_like(dw)
+    w16 = t.empty(1000, dtype=t.bfloat16, device="cuda")
+    for step in (1, 2):
+        _chk(N.lib().pfs_adam(1000, _p(dw), _p(dg), _p(m), _p(v), 1e-2, 0.9, 0.999, 1e-8, step,
+                              0.0, _p(w16), _s()))
+    mm, vv, ww = np.zeros(1000), np.zeros(1000), w.astype(np.float64)
+    for step in (1, 2):
+        mm = 0.9 * mm + 0.1 * g
+        vv = 0.999 * vv + 0.001 * g * g
+        ww = ww - 1e-2 * (mm / (1 - 0.9 ** step)) / (np.sqrt(vv / (1 - 0.999 ** step)) + 1e-8)
+    assert np.allclose(dw.cpu().numpy(), ww, rtol=1e-5, atol=1e-6)
+    assert np.array_equal(w16.float().cpu().numpy(), bf16(dw.cpu().numpy()).astype(np.float32))
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def _cos(a, b):
+    return float(np.sum(a * b) / (np.linalg.norm(a) * np.linalg.norm(b)))
+
+
+def test_network_matches_oracle():
+    """Forward, weight gradients and input gradient of the whole network
+    against the NumPy oracle with the same BF16 operand rounding. The reverse
+    pass rounds each layer's pre-activation gradient to BF16; a value near a
+    rounding tie lands on either side depending on the last bits of the FP32
+    (GPU) or float64 (oracle) sums, so the gradients agree only to a few
+    percent: the oracle itself moves by 3-4 % relative L2 when its GEMMs run
+    in float32 instead of float64. The bounds (6 % relative L2, cosine
+    >= 0.995) sit above that spread; the per-kernel tests above pin each
+    routine tightly."""
+    t = _t()
+    layers = plan()
+    params = init_params(layers, seed=5)
+    params = [(None if w is None else bf16(w), b) for w, b in params]  # BF16-exact weights
+    net = SurrogateNet(32, params=params)
+    rng = np.random.default_rng(6)
+    x = bf16(rng.uniform(-1, 1, (32, 64, 64)))
+    y = net.forward(t.from_numpy(x.astype(np.float32)).cuda()).cpu().numpy().astype(np.float64)
+    ref = RefNet(layers, params, bf16_ops=True)
+    yr = ref.forward(x)
+    assert _rel(y, yr) <= 5e-3, _rel(y, yr)
+    R = rng.standard_normal((32, 32, 2))
+    net.set_output_grad(t.from_numpy(R.astype(np.float32)).cuda())
+    dx = net.backward(input_grad=True).cpu().numpy().astype(np.float64)
+    grads, dxr = ref.backward(R)
+    for li, ((gw, gb), (rw, rb)) in enumerate(zip(net.grads(), grads)):
+        if gw is None:
+            continue
+        assert _rel(gw, rw) <= 6e-2 and _cos(gw, rw) >= 0.995, (li, _rel(gw, rw))
+        assert _rel(gb, rb) <= 6e-2 and _cos(gb, rb) >= 0.995, (li, _rel(gb, rb))
+    assert _rel(dx, dxr) <= 6e-2 and _cos(dx, dxr) >= 0.995, _rel(dx, dxr)
+
+
+def test_training_reduces_loss():
+    """Regression onto a fixed smooth function of the input: 100 Adam steps
+    on the network's own kernels cut the MSE at least two-fold."""
+    t = _t()
+    rng = np.random.default_rng(7)
+    n = 256
+    x = rng.uniform(-1, 1, (n, 64, 64)).astype(np.float32)
+    proj = rng.standard_normal((64, 64, 64)) / 64.0
+    tgt = np.tanh(np.einsum("nij,kij->nk", x, proj)).reshape(n, 32, 2).astype(np.float32)
+    net = SurrogateNet(64, seed=1)
+    dx, dt = t.from_numpy(x).cuda(), t.from_numpy(tgt).cuda()
+    losses = []
+    for step in range(100):
+        sl = slice((step % 4) * 64, (step % 4 + 1) * 64)
+        net.forward(dx[sl])
+        net.loss_grad(dt[sl])
+        losses.append(net.loss_value())
+        net.backward()
+        net.adam_step(2e-3)
+    assert np.isfinite(losses).all()
+    assert np.mean(losses[-4:]) <= np.mean(losses[:4]) / 2, (losses[:4], losses[-4:])
