@@ -23,7 +23,10 @@ PF_CE_CELL1, PF_CE_CELL3, PF_CE_TABLE = 0, 1, 2
 PF_KERNEL_AUTO, PF_KERNEL_SPLIT, PF_KERNEL_FUSED = 0, 1, 2
 
 LIB_NAME = "libpfb200.so"
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
+# PFB200_LIB names another build of the library (same ABI), e.g. one
+# compiled with different tuning macros; default: the in-tree build.
+LIB_PATH = os.environ.get("PFB200_LIB") or os.path.join(
+    os.path.dirname(os.path.abspath(__file__)), LIB_NAME)
 
 _lib: Optional[C.CDLL] = None
 

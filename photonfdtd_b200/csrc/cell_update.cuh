@@ -233,9 +233,18 @@ __device__ __forceinline__ void ade_load(const StepArgs<T>& a, const MediumT<T>*
   r.m = (int)((w >> kMediumShift) & 15u);
   r.loc = w & kLocMask;
   const MediumT<T>& M = media[r.m];
-  const T* R = a.P + M.poff + (long long)r.loc * (6 * M.npole);
-  if (M.npole == 2) ldv<T, 12>(R, r.v);
-  else if (M.npole == 1) ldv<T, 6>(R, r.v);
+  const T* R0 = a.P + M.poff + (long long)r.loc * (3 * M.npole);
+  const T* R1 = R0 + a.plev;
+  if (M.npole == 2) {  // 6 reals per level: 8-byte (f32) / 16-byte (f64) aligned
+    ldv<T, 6>(R0, r.v);
+    ldv<T, 6>(R1, r.v + 6);
+  } else if (M.npole == 1) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      r.v[c] = R0[c];
+      r.v[3 + c] = R1[c];
+    }
+  }
 }
 
 // ADE polarisation update and E correction for one dispersive cell
@@ -271,28 +280,30 @@ __device__ __forceinline__ void ade_update(const StepArgs<T>& a, const MediumT<T
                                            const AdeRec<T>& r, const T en[3], T e[3]) {
   const MediumT<T>& M = media[r.m];
   const int np = M.npole;
-  T* R = a.P + M.poff + (long long)r.loc * (6 * np);
+  T* R = a.P + M.poff + (long long)r.loc * (3 * np);  // level 0 record
   const int lc = a.lvl, lp = a.lvl ^ 1;
+  T* Rc = R + lc * a.plev;
+  T* Rp = R + lp * a.plev;
   if (np == 2) {
     T out[6];
     ade_np<T, 2>(M, r.v, lc, en, e, out);
-    stv<T, 6>(R + lp * 6, out);  // element offset 0 or 6: 8/16-byte aligned
+    stv<T, 6>(Rp, out);
     return;
   }
   if (np == 1) {
     T out[3];
     ade_np<T, 1>(M, r.v, lc, en, e, out);
-    R[lp * 3] = out[0];  // offset 3 is odd: scalar stores
-    R[lp * 3 + 1] = out[1];
-    R[lp * 3 + 2] = out[2];
+    Rp[0] = out[0];
+    Rp[1] = out[1];
+    Rp[2] = out[2];
     return;
   }
   for (int c = 0; c < 3; ++c) {
     T delta = T(0);
     for (int p = 0; p < np; ++p) {
-      const T pc = R[(lc * np + p) * 3 + c], pp = R[(lp * np + p) * 3 + c];
+      const T pc = Rc[p * 3 + c], pp = Rp[p * 3 + c];
       const T pn = add_rn(add_rn(mul_rn(M.a[p], pc), mul_rn(M.b[p], pp)), mul_rn(M.c[p], en[c]));
-      R[(lp * np + p) * 3 + c] = pn;
+      Rp[p * 3 + c] = pn;
       const T inc = sub_rn(pn, pc);
       delta = p == 0 ? inc : add_rn(delta, inc);
     }

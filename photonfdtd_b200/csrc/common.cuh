@@ -71,10 +71,12 @@ constexpr int kMaxMedia = 16;
 constexpr uint32_t kDispersiveBit = 0x80000000u;
 
 // One dispersive medium as the E kernel sees it (simulation.py:572-636).
-// Its polarisation state is one record per cell, at P + poff + loc * 6 * npole,
-// laid out [level 0/1][pole][component]: a cell's state is contiguous, so a
-// warp reads it with a few vector loads. A dispersive cell's word is
-// kDispersiveBit | medium << kMediumShift | loc.
+// Its polarisation state is two arrays, one per time level: level L's record
+// of a cell is at P + L * plev + poff + loc * 3 * npole, laid out
+// [pole][component]. A step reads both levels and rewrites one, so the
+// rewritten records of consecutive cells are contiguous and a warp's stores
+// fill whole sectors (each medium's block starts 8-real aligned). A
+// dispersive cell's word is kDispersiveBit | medium << kMediumShift | loc.
 template <typename T>
 struct MediumT {
   long long poff, count;
@@ -123,7 +125,8 @@ struct StepArgs {
   const MediumT<T>* media;
   int n_media;
   T* P;
-  int lvl;  // polarisation level holding P^n (n & 1)
+  long long plev;  // reals per polarisation level
+  int lvl;         // polarisation level holding P^n (n & 1)
 };
 
 enum CeMode { kCeCell1 = 0, kCeCell3 = 1, kCeTable = 2 };

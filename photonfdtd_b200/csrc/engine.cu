@@ -115,6 +115,7 @@ struct pf_engine {
   void* psiE[6] = {};
   void* psiH[2][6] = {};
   void* P = nullptr;
+  long long plev = 0;  // reals per polarisation level
   void* media = nullptr;
   double* wave = nullptr;
   int* flag = nullptr;
@@ -366,8 +367,8 @@ int finalize_typed(pf_engine* e) {
     for (int lvl = 0; lvl < 2; ++lvl)
       if ((rc = dalloc(e, &e->psiH[lvl][q], eH[q] * S))) return rc;
   }
-  // ADE: per-medium cell records [level][pole][component], each medium's
-  // block aligned to 4 elements so records load with vector loads
+  // ADE: two levels of per-medium cell records [pole][component]; each
+  // medium's block starts 8-real aligned (vector loads, whole-sector stores)
   if (e->n_media > 0) {
     std::vector<MediumT<T>> md(e->n_media);
     long long off = 0;
@@ -375,7 +376,7 @@ int finalize_typed(pf_engine* e) {
     for (int m = 0; m < e->n_media; ++m) {
       MediumT<T>& M = md[m];
       memset(&M, 0, sizeof M);
-      off = (off + 3) & ~3LL;
+      off = (off + 7) & ~7LL;
       M.poff = off;
       M.count = e->m_count[m];
       M.npole = e->m_npole[m];
@@ -386,9 +387,10 @@ int finalize_typed(pf_engine* e) {
         M.b[p] = (T)e->m_coef[ci++];
         M.c[p] = (T)e->m_coef[ci++];
       }
-      off += 6LL * M.npole * M.count;
+      off += 3LL * M.npole * M.count;
     }
-    if ((rc = dalloc(e, &e->P, off * S))) return rc;
+    e->plev = (off + 7) & ~7LL;
+    if ((rc = dalloc(e, &e->P, 2 * e->plev * S))) return rc;
     if ((rc = upload(e, &e->media, md.data(), md.size() * sizeof(MediumT<T>)))) return rc;
     if (e->ce_mode == PF_CE_CELL1)
       if ((rc = upload(e, (void**)&e->adeword, e->h_adeword.data(), n * 4))) return rc;
@@ -486,6 +488,7 @@ StepArgs<T> step_args(pf_engine* e) {
   a.media = (const MediumT<T>*)e->media;
   a.n_media = e->n_media;
   a.P = (T*)e->P;
+  a.plev = e->plev;
   a.lvl = (int)(e->step & 1);
   return a;
 }

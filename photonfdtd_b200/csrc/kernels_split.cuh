@@ -18,6 +18,18 @@
 
 #include "cell3d.cuh"
 
+// Minimum resident 256-thread blocks per SM the split passes are compiled
+// for (register budget 65536 / (256 * n)). Measured on config 3 (384^3 ADE):
+// H at 8 (32 registers, a 12-byte spill) and E at 5 (48 registers) give
+// 1.52 ms of step kernels against 1.77 ms at the compiler's choice (48 / 59
+// registers); E at 6 spills 28 bytes and is slower.
+#ifndef PFB_MINB_H
+#define PFB_MINB_H 8
+#endif
+#ifndef PFB_MINB_E
+#define PFB_MINB_E 5
+#endif
+
 namespace pfb {
 
 // Load f[id + off] only when the neighbour exists (cond), else 0.
@@ -56,7 +68,7 @@ __device__ __forceinline__ bool in_box(int i, int j0, int j1, int k0, int k1, co
 
 // H pass: H^{n+1/2} = H^{n-1/2} - ch (curl E^n + psi).
 template <typename T>
-__global__ void __launch_bounds__(256) k_h_split(const __grid_constant__ StepArgs<T> a) {
+__global__ void __launch_bounds__(256, PFB_MINB_H) k_h_split(const __grid_constant__ StepArgs<T> a) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
@@ -105,7 +117,7 @@ __global__ void __launch_bounds__(256) k_h_split(const __grid_constant__ StepArg
 
 // E pass: E^{n+1} = E^n + ce (curl H^{n+1/2} + psi), then ADE.
 template <typename T, int CE, bool ADE>
-__global__ void __launch_bounds__(256) k_e_split(const __grid_constant__ StepArgs<T> a) {
+__global__ void __launch_bounds__(256, PFB_MINB_E) k_e_split(const __grid_constant__ StepArgs<T> a) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
