@@ -307,6 +307,12 @@ const char *pfs_last_error(void);
  * 16-byte aligned. Tensor cores (BF16 in, FP32 accumulate). */
 int pfs_gemm_bf16(int M, int N, int K, const void *A, int lda, const void *B, int ldb,
                   float *C, int ldc, float alpha, float beta, void *stream);
+/* pfs_gemm_bf16 with the K range split over `splits` blocks along z, for
+ * small M x N and long K (weight gradients): partial products go to `work`
+ * (at least splits * M * N floats) and are added in a fixed order. */
+int pfs_gemm_bf16_splitk(int M, int N, int K, const void *A, int lda, const void *B, int ldb,
+                         float *C, int ldc, float alpha, float beta, int splits, float *work,
+                         int64_t work_floats, void *stream);
 /* Lowering of a 2D convolution (kernel kh x kw, stride, zero padding ph
  * rows / pw columns) over NHWC BF16 input x (nb, H, W, C): col rows
  * (b, oy, ox), columns (ky * kw + kx) * C + c, zero-padded to Kp. */

@@ -64,10 +64,24 @@ __device__ __forceinline__ uint4 ld_chunk(const __nv_bfloat16* p, int rows, int 
 }
 
 // C[M x N] = alpha * sum_k A[m][k] B[n][k] + beta * C. K % 32 == 0; lda, ldb
-// multiples of 8 (16-byte rows); pointers 16-byte aligned.
+// multiples of 8 (16-byte rows); pointers 16-byte aligned. With split-K
+// (gridDim.z > 1) block z sums k in [z * kc, (z + 1) * kc) and writes
+// alpha * partial into its own M x N slab of `work` (leading dimension N);
+// k_splitk_reduce adds the slabs in order.
 __global__ void __launch_bounds__(128) k_gemm_bf16(int M, int N, int K, const __nv_bfloat16* A,
                                                    int lda, const __nv_bfloat16* B, int ldb,
-                                                   float* C, int ldc, float alpha, float beta) {
+                                                   float* C, int ldc, float alpha, float beta,
+                                                   int kc, float* work) {
+  const int kbeg = blockIdx.z * kc;
+  const int kend = min(K, kbeg + kc);
+  if (gridDim.z > 1) {
+    C = work + (long long)blockIdx.z * M * N;
+    ldc = N;
+    beta = 0.f;
+  }
+  A += kbeg;
+  B += kbeg;
+  K = max(0, kend - kbeg);
   __shared__ __align__(16) __nv_bfloat16 As[BM][PADK];
   __shared__ __align__(16) __nv_bfloat16 Bs[BN][PADK];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -86,25 +100,25 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(int M, int N, int K, const __
   uint4 ra[2], rb[2];
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
-    const int q = tid + 128 * h, r = q >> 2, kc = (q & 3) * 8;
-    ra[h] = ld_chunk(A, M, lda, m0 + r, kc);
-    rb[h] = ld_chunk(B, N, ldb, n0 + r, kc);
+    const int q = tid + 128 * h, r = q >> 2, kq = (q & 3) * 8;
+    ra[h] = K > 0 ? ld_chunk(A, M, lda, m0 + r, kq) : make_uint4(0, 0, 0, 0);
+    rb[h] = K > 0 ? ld_chunk(B, N, ldb, n0 + r, kq) : make_uint4(0, 0, 0, 0);
   }
   for (int k0 = 0; k0 < K; k0 += BK) {
     __syncthreads();
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int q = tid + 128 * h, r = q >> 2, kc = (q & 3) * 8;
-      *reinterpret_cast<uint4*>(&As[r][kc]) = ra[h];
-      *reinterpret_cast<uint4*>(&Bs[r][kc]) = rb[h];
+      const int q = tid + 128 * h, r = q >> 2, kq = (q & 3) * 8;
+      *reinterpret_cast<uint4*>(&As[r][kq]) = ra[h];
+      *reinterpret_cast<uint4*>(&Bs[r][kq]) = rb[h];
     }
     __syncthreads();
     if (k0 + BK < K) {
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        const int q = tid + 128 * h, r = q >> 2, kc = (q & 3) * 8;
-        ra[h] = ld_chunk(A, M, lda, m0 + r, k0 + BK + kc);
-        rb[h] = ld_chunk(B, N, ldb, n0 + r, k0 + BK + kc);
+        const int q = tid + 128 * h, r = q >> 2, kq = (q & 3) * 8;
+        ra[h] = ld_chunk(A, M, lda, m0 + r, k0 + BK + kq);
+        rb[h] = ld_chunk(B, N, ldb, n0 + r, k0 + BK + kq);
       }
     }
 #pragma unroll
@@ -144,6 +158,20 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(int M, int N, int K, const __
           *o = beta == 0.f ? v : v + beta * *o;
         }
       }
+}
+
+// C = sum over the split slabs, in order, + beta * C.
+__global__ void k_splitk_reduce(int M, int N, int splits, const float* work, float* C, int ldc,
+                                float beta) {
+  const long long total = (long long)M * N;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int z = 0; z < splits; ++z) s += work[(long long)z * total + t];
+    const long long m = t / N, n = t % N;
+    float* o = C + m * ldc + n;
+    *o = beta == 0.f ? s : s + beta * *o;
+  }
 }
 
 // ---- convolution lowering ----------------------------------------------------
@@ -236,13 +264,20 @@ __global__ void k_act_bwd(long long M, int N, const float* dy, const float* y, i
   }
 }
 
-// dbias[n] = sum over row blocks of part[q][n], in order.
+// dbias[n] = sum over the row blocks of part[q][n]: one block per column,
+// strided partial sums and a fixed-order tree (independent of scheduling).
 __global__ void k_colsum(int R, int N, const float* part, float* out) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= N) return;
+  __shared__ float sh[256];
+  const int n = blockIdx.x;
   float r = 0.f;
-  for (int q = 0; q < R; ++q) r += part[(long long)q * N + n];
-  out[n] = r;
+  for (int q = threadIdx.x; q < R; q += blockDim.x) r += part[(long long)q * N + n];
+  sh[threadIdx.x] = r;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[n] = sh[0];
 }
 
 // out[c][r] = in[r][c] for an R x Cc row-major BF16 matrix; out has leading
@@ -367,9 +402,41 @@ int pfs_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, in
   }
   const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
   if (grid.y > 65535) return sfail(PF_ERR_INVALID, "pfs_gemm_bf16: M too large");
-  k_gemm_bf16<<<grid, 128, 0, (cudaStream_t)stream>>>(
-      M, N, K, (const __nv_bfloat16*)A, lda, (const __nv_bfloat16*)B, ldb, C, ldc, alpha, beta);
+  k_gemm_bf16<<<grid, 128, 0, (cudaStream_t)stream>>>(M, N, K, (const __nv_bfloat16*)A, lda,
+                                                      (const __nv_bfloat16*)B, ldb, C, ldc, alpha,
+                                                      beta, K, nullptr);
   return cuda_status("pfs_gemm_bf16");
+}
+
+int pfs_gemm_bf16_splitk(int M, int N, int K, const void* A, int lda, const void* B, int ldb,
+                         float* C, int ldc, float alpha, float beta, int splits, float* work,
+                         int64_t work_floats, void* stream) {
+  if (splits <= 1) return pfs_gemm_bf16(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, stream);
+  if (M < 0 || N < 0 || K < 1 || (M && N && (!A || !B || !C)) || !work || splits > 65535)
+    return sfail(PF_ERR_INVALID, "pfs_gemm_bf16_splitk: bad sizes or NULL operand");
+  if (K % 32 || lda % 8 || ldb % 8 || lda < K || ldb < K || ldc < N)
+    return sfail(PF_ERR_INVALID,
+                 "pfs_gemm_bf16_splitk: K must be a multiple of 32, lda/ldb multiples of 8");
+  if (!aligned16(A) || !aligned16(B))
+    return sfail(PF_ERR_INVALID, "pfs_gemm_bf16_splitk: A and B must be 16-byte aligned");
+  if ((long long)splits * M * N > work_floats)
+    return sfail(PF_ERR_INVALID, "pfs_gemm_bf16_splitk: work holds fewer than splits*M*N floats");
+  if (!M || !N) return PF_OK;
+  const int kc = ((K + splits - 1) / splits + 31) / 32 * 32;  // multiple of 32
+  const int sz = (K + kc - 1) / kc;
+  const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, sz);
+  if (grid.y > 65535) return sfail(PF_ERR_INVALID, "pfs_gemm_bf16_splitk: M too large");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (sz == 1) {
+    k_gemm_bf16<<<dim3(grid.x, grid.y), 128, 0, st>>>(M, N, K, (const __nv_bfloat16*)A, lda,
+                                                       (const __nv_bfloat16*)B, ldb, C, ldc,
+                                                       alpha, beta, K, nullptr);
+  } else {
+    k_gemm_bf16<<<grid, 128, 0, st>>>(M, N, K, (const __nv_bfloat16*)A, lda,
+                                      (const __nv_bfloat16*)B, ldb, C, ldc, alpha, beta, kc, work);
+    k_splitk_reduce<<<grid_for((long long)M * N, 256), 256, 0, st>>>(M, N, sz, work, C, ldc, beta);
+  }
+  return cuda_status("pfs_gemm_bf16_splitk");
 }
 
 int pfs_im2col(int nb, int H, int W, int C, int kh, int kw, int stride, int ph, int pw,
@@ -414,7 +481,7 @@ int pfs_act_bwd(int64_t M, int N, const float* dy, const float* y, int relu, flo
     return sfail(PF_ERR_INVALID, "pfs_act_bwd: bad arguments");
   k_act_bwd<<<dim3((N + 31) / 32, row_blocks), dim3(32, 8), 0, (cudaStream_t)stream>>>(
       M, N, dy, y, relu, d32, (__nv_bfloat16*)d16, dbias ? part : nullptr);
-  if (dbias) k_colsum<<<(N + 127) / 128, 128, 0, (cudaStream_t)stream>>>(row_blocks, N, part, dbias);
+  if (dbias) k_colsum<<<N, 256, 0, (cudaStream_t)stream>>>(row_blocks, N, part, dbias);
   return cuda_status("pfs_act_bwd");
 }
 

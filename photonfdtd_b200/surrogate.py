@@ -203,6 +203,20 @@ class SurrogateNet:
             self.dx.append(t.zeros((B * L.H * L.W * L.cin,), dtype=f32, device=dev))
             rb = int(min(65535, max(1, M // 64)))
             self.part.append((t.zeros((rb, cp), dtype=f32, device=dev), rb))
+        # split-K for the weight-gradient GEMMs (tiny output, K = all rows)
+        self.splits = []
+        wmax = 0
+        for L in self.layers:
+            if L.kind == "up":
+                self.splits.append(1)
+                continue
+            M = B * L.Ho * L.Wo
+            blocks = -(-L.coutp // 64) * -(-L.Kp // 64)
+            sp = int(max(1, min(-(-296 // blocks), M // 512)))
+            self.splits.append(sp)
+            if sp > 1:
+                wmax = max(wmax, sp * L.coutp * L.Kp)
+        self.work = t.zeros(max(wmax, 1), dtype=f32, device=dev)
         self.x16 = t.zeros((B, 64, 64), dtype=bf, device=dev)
         self.gout = t.zeros((B * N_FREQ, 32), dtype=f32, device=dev)
         self.loss_parts = t.zeros(64, dtype=f32, device=dev)
@@ -284,9 +298,10 @@ class SurrogateNet:
                                             self._p(self.dT[li]), M, s))
             self._chk(L_.pfs_transpose_bf16(M, L.Kp, self._p(A), L.Kp, self._p(self.colT[li]), M,
                                             s))
-            self._chk(L_.pfs_gemm_bf16(L.coutp, L.Kp, M, self._p(self.dT[li]), M,
-                                       self._p(self.colT[li]), M, self._p(self.gw[li]), L.Kp,
-                                       1.0, 0.0, s))
+            self._chk(L_.pfs_gemm_bf16_splitk(L.coutp, L.Kp, M, self._p(self.dT[li]), M,
+                                              self._p(self.colT[li]), M, self._p(self.gw[li]),
+                                              L.Kp, 1.0, 0.0, self.splits[li],
+                                              self._p(self.work), self.work.numel(), s))
             if first and not input_grad:
                 break
             # input gradient: dcol = d W, then col2im

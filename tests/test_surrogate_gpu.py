@@ -47,6 +47,32 @@ def test_gemm_bf16(M, Nn, K, beta):
     assert np.max(np.abs(got - want)) <= 1e-5 * np.max(np.abs(want)) * np.sqrt(K)
 
 
+@pytest.mark.parametrize("M,Nn,K,splits,beta", [(32, 64, 65536, 64, 0.0), (64, 32, 4096, 7, 1.0),
+                                                 (100, 40, 96, 3, 0.5)])
+def test_gemm_bf16_splitk(M, Nn, K, splits, beta):
+    """Split-K (long K, small output: the weight gradients) against NumPy and
+    bitwise against itself on a second call (fixed reduction order)."""
+    t = _t()
+    rng = np.random.default_rng(K + splits)
+    A = bf16(rng.standard_normal((M, K)))
+    B = bf16(rng.standard_normal((Nn, K)))
+    C0 = rng.standard_normal((M, Nn)).astype(np.float32)
+    dA = t.from_numpy(A.astype(np.float32)).cuda().to(t.bfloat16)
+    dB = t.from_numpy(B.astype(np.float32)).cuda().to(t.bfloat16)
+    work = t.empty(splits * M * Nn, dtype=t.float32, device="cuda")
+    outs = []
+    for _ in range(2):
+        dC = t.from_numpy(C0.copy()).cuda()
+        _chk(N.lib().pfs_gemm_bf16_splitk(M, Nn, K, _p(dA), K, _p(dB), K, _p(dC), Nn, 1.0, beta,
+                                          splits, _p(work), work.numel(), _s()))
+        outs.append(dC.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1])
+    want = A @ B.T + beta * C0
+    assert np.max(np.abs(outs[0] - want)) <= 1e-5 * np.max(np.abs(want)) * np.sqrt(K)
+    assert N.lib().pfs_gemm_bf16_splitk(M, Nn, K, _p(dA), K, _p(dB), K, _p(dC), Nn, 1.0, beta,
+                                        splits, _p(work), 10, _s()) == N.PF_ERR_INVALID
+
+
 def test_gemm_rejects_bad_shapes():
     L = N.lib()
     assert L.pfs_gemm_bf16(4, 4, 20, 16, 20, 16, 20, 16, 4, 1.0, 0.0, None) == N.PF_ERR_INVALID
