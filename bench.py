@@ -63,6 +63,10 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--adjoint-iters", type=int, default=2)
+    p.add_argument("--only-adjoint", action="store_true",
+                   help="time the config-4 gradient iteration alone (profiling)")
+    p.add_argument("--adjoint-instances", type=int, default=256)
+    p.add_argument("--adjoint-steps", type=int, default=4000)
     return p.parse_args()
 
 
@@ -225,15 +229,15 @@ ADJ_WORKLOAD = ("config4: 256 2D TE instances, nx ~U{200..800} x ny ~U{150..400}
                 "8 wavelengths on the output line, 4000 steps forward + discrete adjoint")
 
 
-def adjoint_bench(iters: int, cpu: bool):
+def adjoint_bench(iters: int, cpu: bool, n_inst: int = 256, n_steps: int = 4000):
     """Seconds per gradient iteration of the config-4 batch: set the design,
     forward, read the line DFT, cotangent of J = sum |F|^2, adjoint, read
     dJ/deps - one value_and_grad_eps call, wall clock on the host."""
     import photonfdtd_b200 as pf
     from photonfdtd_b200 import workloads as W
     from photonfdtd_b200.batch import BatchTE, value_and_grad_eps
-    sizes = W.config4_sizes()
-    sims = [W.config4_instance(pf, nx, ny, i=k) for k, (nx, ny) in enumerate(sizes)]
+    sizes = W.config4_sizes()[:n_inst]
+    sims = [W.config4_instance(pf, nx, ny, i=k, n_steps=n_steps) for k, (nx, ny) in enumerate(sizes)]
     wins = [W.design_window_box(nx, ny, 64) for nx, ny in sizes]
     t0 = time.perf_counter()
     b = BatchTE(sims, wins)
@@ -289,6 +293,11 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.only_adjoint:
+        adj = adjoint_bench(max(1, args.adjoint_iters), False, args.adjoint_instances,
+                            args.adjoint_steps)
+        print(json.dumps(adj), flush=True)
+        return
     import torch
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
