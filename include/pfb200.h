@@ -313,6 +313,14 @@ int pfs_gemm_bf16(int M, int N, int K, const void *A, int lda, const void *B, in
 int pfs_gemm_bf16_splitk(int M, int N, int K, const void *A, int lda, const void *B, int ldb,
                          float *C, int ldc, float alpha, float beta, int splits, float *work,
                          int64_t work_floats, void *stream);
+/* Selects the tensor-core engine of the two GEMM entry points for the
+ * process: 1 = tcgen05.mma with the accumulator in tensor memory (default),
+ * 0 = mma.sync m16n8k16 with register accumulators. Other values only query.
+ * Returns the previous engine. */
+int pfs_gemm_engine(int engine);
+/* Number of tcgen05 GEMM blocks whose bounded wait for their MMAs ran out
+ * (their output tile is then not written); reset = 1 clears it. Synchronous. */
+int pfs_gemm_timeouts(int *count, int reset);
 /* Lowering of a 2D convolution (kernel kh x kw, stride, zero padding ph
  * rows / pw columns) over NHWC BF16 input x (nb, H, W, C): col rows
  * (b, oy, ox), columns (ky * kw + kx) * C + c, zero-padded to Kp. */

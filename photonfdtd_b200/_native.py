@@ -94,6 +94,8 @@ SIGNATURES = {
     "pfs_gemm_bf16_splitk": (C.c_int, [C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int,
                                        _vp, C.c_int, C.c_float, C.c_float, C.c_int, _vp, _i64,
                                        _vp]),
+    "pfs_gemm_engine": (C.c_int, [C.c_int]),
+    "pfs_gemm_timeouts": (C.c_int, [C.POINTER(C.c_int), C.c_int]),
     "pfs_im2col": (C.c_int, [C.c_int] * 9 + [_vp, _vp, C.c_int, _vp]),
     "pfs_col2im": (C.c_int, [C.c_int] * 9 + [_vp, C.c_int, _vp, _vp]),
     "pfs_bias_act": (C.c_int, [_i64, C.c_int, _vp, _vp, C.c_int, _vp, _vp, _vp]),

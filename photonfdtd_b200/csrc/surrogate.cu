@@ -18,6 +18,7 @@
 //     Adam step on FP32 master weights that refreshes their BF16 copies.
 // Activations are NHWC. Nothing here allocates: the caller owns every buffer
 // and passes its stream (NULL = the default stream).
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -158,6 +159,237 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(int M, int N, int K, const __
           *o = beta == 0.f ? v : v + beta * *o;
         }
       }
+}
+
+// ---- tcgen05 GEMM ------------------------------------------------------------
+// The same contract as k_gemm_bf16 on the 5th-generation tensor cores: a
+// 128 x BN output tile per CTA accumulates in tensor memory (TMEM, BN 32-bit
+// columns x 128 lanes) from tcgen05.mma.cta_group::1.kind::f16 (BF16 in, FP32
+// accumulate). Operand tiles of 64 K-columns (128-byte rows) arrive by TMA
+// (cp.async.bulk.tensor, 128-byte swizzle, zeros past the matrix edge) in a
+// ring of TC_STAGES stages: warp 0 produces (waits for a stage's `empty`
+// barrier, posts the byte count on its `full` barrier, issues the two loads),
+// warp 1 consumes (waits for `full`, lane 0 issues four K = 16 MMAs and
+// commits them to `empty`, so the stage is refilled once they have read it).
+// A last commit to `done` releases all four warps into the epilogue: each
+// reads its 32 TMEM lanes (tile rows) with tcgen05.ld.32x32b, transposes
+// 32 x 32 blocks through shared memory and stores whole rows.
+// Shared-memory descriptor of a K-major 128-byte-swizzled operand: rows at
+// 128 bytes, 8-row groups at 1024 bytes (stride byte offset), leading byte
+// offset unused (1), layout type 2; the K = 16 slice ks of a stage starts
+// 32 * ks bytes into each row (the swizzle is applied to the full address,
+// so stage bases are 1024-byte aligned).
+// Every wait is bounded (kTcWaitNs): on a timeout the block sets an abort
+// flag, waits (bounded) for its own loads and MMAs in flight, records the
+// timeout in *err, skips the epilogue, frees its TMEM and returns.
+constexpr int TBM = 128, TBK = 64, TC_STAGES = 4;
+constexpr unsigned long long kTcWaitNs = 1000000000ull;  // 1 s per wait
+
+__host__ __device__ constexpr int tc_stage_bytes(int bn) { return (TBM + bn) * TBK * 2; }
+__host__ __device__ constexpr int tc_smem_bytes(int bn) {
+  return TC_STAGES * tc_stage_bytes(bn) + 1024;  // + alignment of the ring to 1024 bytes
+}
+
+__device__ __forceinline__ unsigned long long tc_now() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ bool tc_mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.b32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for the completion of the phase with the given parity, at most
+// kTcWaitNs (and at most 2^30 polls); gives up early once *abort is set.
+__device__ __forceinline__ bool tc_mbar_wait(uint32_t bar, uint32_t parity,
+                                             const volatile int* abort = nullptr) {
+  const unsigned long long t0 = tc_now();
+  for (int i = 0; i < (1 << 30); ++i) {
+    if (tc_mbar_try(bar, parity)) return true;
+    if ((i & 63) == 63 && (tc_now() - t0 > kTcWaitNs || (abort && *abort))) return false;
+  }
+  return false;
+}
+
+__device__ __forceinline__ uint64_t tc_desc_sw128(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         (1ull << 46) | (2ull << 61);
+}
+
+__device__ __forceinline__ void tc_tma_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar,
+                                          int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+      "l"((unsigned long long)map), "r"(bar), "r"(x), "r"(y)
+      : "memory");
+}
+
+template <int BN>
+__global__ void __launch_bounds__(128, 1)
+    k_gemm_tc(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
+              int M, int N, int K, float* C, int ldc, float alpha, float beta, int kc, float* work,
+              int* err) {
+  static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "BN");
+  constexpr uint32_t ABYTES = TBM * TBK * 2, SB = tc_stage_bytes(BN);
+  extern __shared__ uint8_t tc_smem[];
+  __shared__ __align__(8) uint64_t full[TC_STAGES], empty[TC_STAGES], done;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag, n_loaded, n_seen;
+  volatile int* abort_v = &abort_flag;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.y * TBM, n0 = blockIdx.x * BN;
+  const int kbeg = blockIdx.z * kc;
+  const int kend = min(K, kbeg + kc);
+  if (gridDim.z > 1) {
+    C = work + (long long)blockIdx.z * M * N;
+    ldc = N;
+    beta = 0.f;
+  }
+  const int nk = (kend - kbeg + TBK - 1) / TBK;  // >= 1 (host guarantees non-empty slices)
+  const uint32_t s0 = (smem_u32(tc_smem) + 1023u) & ~1023u;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_slot)),
+                 "r"(BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 32) {
+    for (int i = 0; i < TC_STAGES; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[i])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[i])));
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&done)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    abort_flag = 0;
+    n_loaded = 0;
+    n_seen = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tmem_slot;
+  if (warp == 0) {  // producer
+    int kt = 0;
+    for (; kt < nk; ++kt) {
+      const int st = kt % TC_STAGES;
+      bool ok = true;
+      if (kt >= TC_STAGES)
+        ok = tc_mbar_wait(smem_u32(&empty[st]), ((kt / TC_STAGES) - 1) & 1, abort_v);
+      if (!__all_sync(0xffffffffu, ok && !*abort_v)) {
+        if (lane == 0) *abort_v = 1;
+        break;
+      }
+      if (lane == 0) {
+        const uint32_t fb = smem_u32(&full[st]), dst = s0 + st * SB;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(SB)
+                     : "memory");
+        tc_tma_2d(dst, &ta, fb, kbeg + kt * TBK, m0);
+        tc_tma_2d(dst + ABYTES, &tb, fb, kbeg + kt * TBK, n0);
+      }
+      __syncwarp();
+    }
+    if (lane == 0) n_loaded = kt;
+  } else if (warp == 1) {  // MMA issue
+    constexpr uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) |
+                               ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TBM >> 4) << 24);
+    int kt = 0;
+    for (; kt < nk; ++kt) {
+      const int st = kt % TC_STAGES;
+      const bool ok = tc_mbar_wait(smem_u32(&full[st]), (kt / TC_STAGES) & 1, abort_v);
+      if (!__all_sync(0xffffffffu, ok && !*abort_v)) {
+        if (lane == 0) *abort_v = 1;
+        break;
+      }
+      if (lane == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t a0 = s0 + st * SB, b0 = a0 + ABYTES;
+#pragma unroll
+        for (int ks = 0; ks < TBK / 16; ++ks) {
+          const uint64_t da = tc_desc_sw128(a0 + 32 * ks), db = tc_desc_sw128(b0 + 32 * ks);
+          const uint32_t accum = (kt > 0 || ks > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::
+                  "r"(tmem),
+              "l"(da), "l"(db), "r"(idesc), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+        }
+        asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                smem_u32(&empty[st])));
+      }
+      __syncwarp();
+    }
+    if (lane == 0) {
+      n_seen = kt;
+      // covers every MMA issued above (arrives at once if there were none)
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              smem_u32(&done)));
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  bool ok = tc_mbar_wait(smem_u32(&done), 0);
+  if (__syncthreads_or(!ok || abort_flag)) {
+    // loads issued but never consumed are still in flight: wait for them
+    if (tid == 0) {
+      for (int kt = n_seen; kt < n_loaded; ++kt)
+        tc_mbar_wait(smem_u32(&full[kt % TC_STAGES]), (kt / TC_STAGES) & 1);
+      atomicExch(err, 1);
+    }
+  } else {
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    float* stage = reinterpret_cast<float*>(tc_smem + (s0 - smem_u32(tc_smem))) + warp * 32 * 33;
+    const int rbase = m0 + warp * 32;
+#pragma unroll 1
+    for (int cb = 0; cb < BN / 32; ++cb) {
+      if (n0 + cb * 32 >= N) break;  // uniform
+      uint32_t v[32];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cb * 32);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
+          "%10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, "
+          "%27, %28, %29, %30, %31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+            "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+            "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+            "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+            "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+            "=r"(v[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int j = 0; j < 32; ++j) stage[lane * 33 + j] = __uint_as_float(v[j]);
+      __syncwarp();
+      const int n = n0 + cb * 32 + lane;
+      for (int rr = 0; rr < 32; ++rr) {
+        const int r = rbase + rr;
+        if (r < M && n < N) {
+          float* o = C + (long long)r * ldc + n;
+          const float val = alpha * stage[rr * 33 + lane];
+          *o = beta == 0.f ? val : val + beta * *o;
+        }
+      }
+      __syncwarp();
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
 }
 
 // C = sum over the split slabs, in order, + beta * C.
@@ -373,6 +605,94 @@ __global__ void k_adam(long long n, float* w, const float* g, float* m, float* v
   }
 }
 
+__device__ int g_tc_err = 0;
+
+typedef CUresult (*TcEncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                               const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                               const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                               CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// TMA map of a row-major BF16 matrix (rows x cols, leading dimension ld
+// elements), box 64 columns x box_rows rows, 128-byte swizzle, zeros outside.
+bool tc_map(CUtensorMap* m, const void* ptr, int cols, int rows, int ld, int box_rows) {
+  static TcEncodeFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return false;
+    fn = (TcEncodeFn)p;
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)TBK, (cuuint32_t)box_rows};
+  const cuuint32_t es[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+int g_gemm_engine = 1;  // 1: tcgen05 (TMEM accumulator), 0: mma.sync m16n8k16
+
+// Launches the GEMM (split over `sz` K slices of kc when sz > 1).
+int launch_gemm(int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B,
+                int ldb, float* C, int ldc, float alpha, float beta, int kc, int sz, float* work,
+                cudaStream_t st) {
+  if (g_gemm_engine == 0) {
+    const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, sz);
+    if (grid.y > 65535) return sfail(PF_ERR_INVALID, "pfs_gemm: M too large");
+    k_gemm_bf16<<<grid, 128, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, kc, work);
+    return PF_OK;
+  }
+  static int* err = nullptr;
+  if (!err && cudaGetSymbolAddress((void**)&err, g_tc_err) != cudaSuccess)
+    return sfail(PF_ERR_CUDA, "pfs_gemm: cannot resolve the tensor-core error flag");
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_gemm_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             tc_smem_bytes(256)) != cudaSuccess ||
+        cudaFuncSetAttribute(k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             tc_smem_bytes(128)) != cudaSuccess ||
+        cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             tc_smem_bytes(64)) != cudaSuccess ||
+        cudaFuncSetAttribute(k_gemm_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             tc_smem_bytes(32)) != cudaSuccess)
+      return cuda_status("pfs_gemm: shared memory attribute");
+    attr = true;
+  }
+  if (sz == 1) kc = (K + TBK - 1) / TBK * TBK;  // one slice: the whole K range
+  if (kc % TBK) return sfail(PF_ERR_INVALID, "pfs_gemm: K slice not a multiple of 64");
+  const long long gy = (M + TBM - 1) / TBM;
+  if (gy > 65535) return sfail(PF_ERR_INVALID, "pfs_gemm: M too large");
+  // the narrowest tile that covers N, narrowed further (down to 32 columns)
+  // while the grid has fewer blocks than SMs
+  int bn = N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
+  while (bn > 32 && gy * ((N + bn - 1) / bn) * sz < 148) bn /= 2;
+  CUtensorMap ta, tb;
+  if (!tc_map(&ta, A, K, M, lda, TBM) || !tc_map(&tb, B, K, N, ldb, bn))
+    return sfail(PF_ERR_CUDA, "pfs_gemm: cuTensorMapEncodeTiled failed");
+  const dim3 grid((N + bn - 1) / bn, (unsigned)gy, sz);
+  switch (bn) {
+    case 32:
+      k_gemm_tc<32><<<grid, 128, tc_smem_bytes(32), st>>>(ta, tb, M, N, K, C, ldc, alpha, beta,
+                                                          kc, work, err);
+      break;
+    case 64:
+      k_gemm_tc<64><<<grid, 128, tc_smem_bytes(64), st>>>(ta, tb, M, N, K, C, ldc, alpha, beta,
+                                                          kc, work, err);
+      break;
+    case 128:
+      k_gemm_tc<128><<<grid, 128, tc_smem_bytes(128), st>>>(ta, tb, M, N, K, C, ldc, alpha, beta,
+                                                            kc, work, err);
+      break;
+    default:
+      k_gemm_tc<256><<<grid, 128, tc_smem_bytes(256), st>>>(ta, tb, M, N, K, C, ldc, alpha, beta,
+                                                            kc, work, err);
+  }
+  return PF_OK;
+}
+
 unsigned grid_for(long long n, int block) {
   long long g = (n + block - 1) / block;
   if (g > 148LL * 32) g = 148LL * 32;
@@ -387,6 +707,24 @@ extern "C" {
 
 const char* pfs_last_error(void) { return g_err.c_str(); }
 
+int pfs_gemm_engine(int engine) {
+  const int old = g_gemm_engine;
+  if (engine == 0 || engine == 1) g_gemm_engine = engine;
+  return old;
+}
+
+int pfs_gemm_timeouts(int* count, int reset) {
+  if (!count) return sfail(PF_ERR_INVALID, "pfs_gemm_timeouts: NULL");
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_tc_err, sizeof v) != cudaSuccess) return cuda_status("pfs_gemm_timeouts");
+  if (reset) {
+    const int z = 0;
+    if (cudaMemcpyToSymbol(g_tc_err, &z, sizeof z) != cudaSuccess) return cuda_status("pfs_gemm_timeouts");
+  }
+  *count = v;
+  return PF_OK;
+}
+
 int pfs_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C,
                   int ldc, float alpha, float beta, void* stream) {
   if (M < 0 || N < 0 || K < 0 || (M && N && (!A || !B || !C)))
@@ -400,11 +738,9 @@ int pfs_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, in
   if (K == 0) {
     return sfail(PF_ERR_INVALID, "pfs_gemm_bf16: K must be positive");
   }
-  const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-  if (grid.y > 65535) return sfail(PF_ERR_INVALID, "pfs_gemm_bf16: M too large");
-  k_gemm_bf16<<<grid, 128, 0, (cudaStream_t)stream>>>(M, N, K, (const __nv_bfloat16*)A, lda,
-                                                      (const __nv_bfloat16*)B, ldb, C, ldc, alpha,
-                                                      beta, K, nullptr);
+  const int rc = launch_gemm(M, N, K, (const __nv_bfloat16*)A, lda, (const __nv_bfloat16*)B, ldb,
+                             C, ldc, alpha, beta, K, 1, nullptr, (cudaStream_t)stream);
+  if (rc) return rc;
   return cuda_status("pfs_gemm_bf16");
 }
 
@@ -422,20 +758,22 @@ int pfs_gemm_bf16_splitk(int M, int N, int K, const void* A, int lda, const void
   if ((long long)splits * M * N > work_floats)
     return sfail(PF_ERR_INVALID, "pfs_gemm_bf16_splitk: work holds fewer than splits*M*N floats");
   if (!M || !N) return PF_OK;
-  const int kc = ((K + splits - 1) / splits + 31) / 32 * 32;  // multiple of 32
-  const int sz = (K + kc - 1) / kc;
-  const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, sz);
-  if (grid.y > 65535) return sfail(PF_ERR_INVALID, "pfs_gemm_bf16_splitk: M too large");
+  const int g = g_gemm_engine ? TBK : 32;  // K-tile of the engine
+  const int kc = ((K + splits - 1) / splits + g - 1) / g * g;
+  const int sz = (K + kc - 1) / kc;  // every slice non-empty
   cudaStream_t st = (cudaStream_t)stream;
+  int rc;
   if (sz == 1) {
-    k_gemm_bf16<<<dim3(grid.x, grid.y), 128, 0, st>>>(M, N, K, (const __nv_bfloat16*)A, lda,
-                                                       (const __nv_bfloat16*)B, ldb, C, ldc,
-                                                       alpha, beta, K, nullptr);
+    rc = launch_gemm(M, N, K, (const __nv_bfloat16*)A, lda, (const __nv_bfloat16*)B, ldb, C, ldc,
+                     alpha, beta, K, 1, nullptr, st);
   } else {
-    k_gemm_bf16<<<grid, 128, 0, st>>>(M, N, K, (const __nv_bfloat16*)A, lda,
-                                      (const __nv_bfloat16*)B, ldb, C, ldc, alpha, beta, kc, work);
-    k_splitk_reduce<<<grid_for((long long)M * N, 256), 256, 0, st>>>(M, N, sz, work, C, ldc, beta);
+    rc = launch_gemm(M, N, K, (const __nv_bfloat16*)A, lda, (const __nv_bfloat16*)B, ldb, C, ldc,
+                     alpha, beta, kc, sz, work, st);
+    if (!rc)
+      k_splitk_reduce<<<grid_for((long long)M * N, 256), 256, 0, st>>>(M, N, sz, work, C, ldc,
+                                                                        beta);
   }
+  if (rc) return rc;
   return cuda_status("pfs_gemm_bf16_splitk");
 }
 

@@ -43,6 +43,8 @@ def main(argv=None):
     p.add_argument("--wd", type=float, default=0.05)
     p.add_argument("--profile-steps", type=int, default=0,
                    help="only time this many training steps on random inputs (batch --batch)")
+    p.add_argument("--gemm-engine", type=int, default=1, choices=(0, 1),
+                   help="tensor-core GEMM engine: 1 tcgen05 (default), 0 mma.sync")
     p.add_argument("--data", default=None,
                    help="npz of cached spectra (T_train, T_heldout); written if absent")
     a = p.parse_args(argv)
@@ -50,6 +52,8 @@ def main(argv=None):
     from . import surrogate as S
     os.makedirs(a.out, exist_ok=True)
     rep = {}
+    from . import _native as N
+    N.lib().pfs_gemm_engine(a.gemm_engine)
     if a.profile_steps:
         net = S.SurrogateNet(a.batch)
         x = torch.rand(a.batch, 64, 64, device="cuda") * 2 - 1
@@ -62,9 +66,9 @@ def main(argv=None):
             net.forward(x); net.loss_grad(t); net.backward(); net.adam_step(1e-3)
         e1.record()
         torch.cuda.synchronize()
-        out = {"batch": a.batch, "train_step_ms": e0.elapsed_time(e1) / a.profile_steps}
+        out = {"batch": a.batch, "gemm_engine": a.gemm_engine,
+               "train_step_ms": e0.elapsed_time(e1) / a.profile_steps}
         # the GEMM kernel alone: a square case and the largest forward layers
-        from . import _native as N
         L = N.lib()
         st = torch.cuda.current_stream().cuda_stream
         for (M, Nn, K) in [(8192, 8192, 8192), (a.batch * 64, 256, 1152),

@@ -3,6 +3,8 @@ FP32-accumulation accuracy, the convolution lowering and its adjoint, the
 elementwise / reduction kernels, Adam, and the whole network's forward and
 reverse pass against the NumPy oracle (oracle/surrogate_ref.py) run with the
 same BF16 rounding of GEMM operands. A short training run must cut the loss."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -30,9 +32,25 @@ def _s():
     return _t().cuda.current_stream().cuda_stream
 
 
+@pytest.fixture(params=[1, 0], ids=["tcgen05", "mma_sync"])
+def engine(request):
+    """Runs a GEMM test on each tensor-core engine and checks that no tcgen05
+    block ran out of its bounded wait."""
+    L = N.lib()
+    old = L.pfs_gemm_engine(request.param)
+    cnt = C.c_int(0)
+    _chk(L.pfs_gemm_timeouts(C.byref(cnt), 1))
+    yield request.param
+    _chk(L.pfs_gemm_timeouts(C.byref(cnt), 1))
+    L.pfs_gemm_engine(old)
+    assert cnt.value == 0
+
+
 @pytest.mark.parametrize("M,Nn,K,beta", [(100, 70, 96, 0.0), (257, 33, 32, 0.5),
-                                          (64, 512, 2048, 0.0), (4096, 32, 32, 1.0)])
-def test_gemm_bf16(M, Nn, K, beta):
+                                          (64, 512, 2048, 0.0), (4096, 32, 32, 1.0),
+                                          (128, 128, 64, 0.0), (300, 200, 160, 0.25),
+                                          (129, 8, 32, 0.0), (1000, 96, 544, 1.0)])
+def test_gemm_bf16(M, Nn, K, beta, engine):
     t = _t()
     rng = np.random.default_rng(M + Nn + K)
     A = bf16(rng.standard_normal((M, K)))
@@ -49,7 +67,7 @@ def test_gemm_bf16(M, Nn, K, beta):
 
 @pytest.mark.parametrize("M,Nn,K,splits,beta", [(32, 64, 65536, 64, 0.0), (64, 32, 4096, 7, 1.0),
                                                  (100, 40, 96, 3, 0.5)])
-def test_gemm_bf16_splitk(M, Nn, K, splits, beta):
+def test_gemm_bf16_splitk(M, Nn, K, splits, beta, engine):
     """Split-K (long K, small output: the weight gradients) against NumPy and
     bitwise against itself on a second call (fixed reduction order)."""
     t = _t()
