@@ -313,6 +313,40 @@ __device__ __forceinline__ void ade_update(const StepArgs<T>& a, const MediumT<T
 
 // E-update coefficients of one cell and, for a dispersive cell, its ADE
 // word (0 for a plain cell).
+// cell_coeffs in two halves, so that a kernel can issue its other loads
+// between them: cell_word issues the per-cell loads (coefficient or table
+// word), cell_decode turns them into K and the ADE word (table lookups).
+template <typename T, int CE, bool ADE>
+__device__ __forceinline__ void cell_word(const StepArgs<T>& a, long long id, T K[3],
+                                          uint32_t& t) {
+  t = 0u;
+  if (CE == kCeCell1) {
+    K[0] = K[1] = K[2] = a.ce[0][id];
+    if (ADE) t = a.adeword[id];
+  } else if (CE == kCeCell3) {
+    K[0] = a.ce[0][id];
+    K[1] = a.ce[1][id];
+    K[2] = a.ce[2][id];
+  } else {
+    t = a.word[id];
+  }
+}
+template <typename T, int CE, bool ADE>
+__device__ __forceinline__ void cell_decode(const StepArgs<T>& a, const MediumT<T>* media,
+                                            uint32_t t, T K[3], uint32_t& w) {
+  w = 0u;
+  if (CE == kCeCell1) {
+    w = t;
+  } else if (CE == kCeTable) {
+    if (ADE && (t & kDispersiveBit)) {
+      w = t;
+      K[0] = K[1] = K[2] = media[(t >> kMediumShift) & 15u].ce;
+    } else {
+      K[0] = K[1] = K[2] = a.table[t & ~kDispersiveBit];
+    }
+  }
+}
+
 template <typename T, int CE, bool ADE>
 __device__ __forceinline__ void cell_coeffs(const StepArgs<T>& a, const MediumT<T>* media,
                                             long long id, T K[3], uint32_t& w) {

@@ -126,27 +126,46 @@ __global__ void __launch_bounds__(256, PFB_MINB_E) k_e_split(const __grid_consta
   if (k >= a.nz || j >= a.ny) return;
   const long long sy = a.nz, sx = (long long)a.ny * a.nz;
   const long long id = i * sx + j * sy + k;
+  // Loads are issued in dependency order: the per-cell word and every field
+  // value first, then what the word selects (table coefficient, ADE record),
+  // so a warp waits out two memory latencies, not three.
   T K[3];
-  uint32_t w;
-  cell_coeffs<T, CE, ADE>(a, a.media, id, K, w);
-  AdeRec<T> rec;
-  if (ADE && w) ade_load<T>(a, a.media, w, rec);
+  uint32_t t, w;
+  cell_word<T, CE, ADE>(a, id, K, t);
   const T hx = a.Hin[0][id], hy = a.Hin[1][id], hz = a.Hin[2][id];
   T en[3] = {a.Ein[0][id], a.Ein[1][id], a.Ein[2][id]};
-  T e[3];
+  const bool d3 = a.nx > 1 && a.ny > 1 && a.nz > 1;
+  T hn[6];  // Hz(j-1), Hy(k-1), Hx(k-1), Hz(i-1), Hy(i-1), Hx(j-1); 3D grids only
   if (box) {
-    // Ex: +dHz/dy - dHy/dz; Ey: +dHx/dz - dHz/dx; Ez: +dHy/dx - dHx/dy
-    const T n[6] = {sub_rn(hz, a.Hin[2][id - sy]), sub_rn(hy, a.Hin[1][id - 1]),
-                    sub_rn(hx, a.Hin[0][id - 1]), sub_rn(hz, a.Hin[2][id - sx]),
-                    sub_rn(hy, a.Hin[1][id - sx]), sub_rn(hx, a.Hin[0][id - sy])};
-    const int ax[6] = {1, 2, 2, 0, 0, 1};
-    bulk3<T>(a, en, K, n, ax, e);
-  } else if (a.nx > 1 && a.ny > 1 && a.nz > 1) {
+    hn[0] = a.Hin[2][id - sy];
+    hn[1] = a.Hin[1][id - 1];
+    hn[2] = a.Hin[0][id - 1];
+    hn[3] = a.Hin[2][id - sx];
+    hn[4] = a.Hin[1][id - sx];
+    hn[5] = a.Hin[0][id - sy];
+  } else if (d3) {
     const bool lx = i > 0, ly = j > 0, lz = k > 0;
-    const T n[6] = {sub_rn(hz, ld_if(a.Hin[2], id, -sy, ly)), sub_rn(hy, ld_if(a.Hin[1], id, -1, lz)),
-                    sub_rn(hx, ld_if(a.Hin[0], id, -1, lz)), sub_rn(hz, ld_if(a.Hin[2], id, -sx, lx)),
-                    sub_rn(hy, ld_if(a.Hin[1], id, -sx, lx)), sub_rn(hx, ld_if(a.Hin[0], id, -sy, ly))};
-    e3<T>(a, i, j, k, en, K, n, e);
+    hn[0] = ld_if(a.Hin[2], id, -sy, ly);
+    hn[1] = ld_if(a.Hin[1], id, -1, lz);
+    hn[2] = ld_if(a.Hin[0], id, -1, lz);
+    hn[3] = ld_if(a.Hin[2], id, -sx, lx);
+    hn[4] = ld_if(a.Hin[1], id, -sx, lx);
+    hn[5] = ld_if(a.Hin[0], id, -sy, ly);
+  }
+  cell_decode<T, CE, ADE>(a, a.media, t, K, w);
+  AdeRec<T> rec;
+  if (ADE && w) ade_load<T>(a, a.media, w, rec);
+  T e[3];
+  if (box || d3) {
+    // Ex: +dHz/dy - dHy/dz; Ey: +dHx/dz - dHz/dx; Ez: +dHy/dx - dHx/dy
+    const T n[6] = {sub_rn(hz, hn[0]), sub_rn(hy, hn[1]), sub_rn(hx, hn[2]),
+                    sub_rn(hz, hn[3]), sub_rn(hy, hn[4]), sub_rn(hx, hn[5])};
+    if (box) {
+      const int ax[6] = {1, 2, 2, 0, 0, 1};
+      bulk3<T>(a, en, K, n, ax, e);
+    } else {
+      e3<T>(a, i, j, k, en, K, n, e);
+    }
   } else {
     const bool lx = i > 0, ly = j > 0, lz = k > 0;
     e[0] = upd_ex<T>(a, i, j, k, en[0], K[0], hz, ld_if(a.Hin[2], id, -sy, ly), hy,
