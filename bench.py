@@ -61,6 +61,8 @@ def parse():
     p.add_argument("--size", type=int, default=384, help="cells per axis (default 384)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-surrogate", action="store_true",
+                   help="skip the surrogate tensor-core GEMM / training-step figures")
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--adjoint-iters", type=int, default=2)
     p.add_argument("--only-adjoint", action="store_true",
@@ -177,6 +179,31 @@ def peaks():
         return float(p["hbm_gbs"]), "measured"
     except (OSError, KeyError, ValueError):
         return 6650.0, "fallback"
+
+
+def bf16_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured (burst)"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
+
+
+def surrogate_bench():
+    """The surrogate's tensor-core GEMM (tcgen05, TMEM accumulator) against
+    the measured bf16 peak, on a square case and on the network's largest
+    layer (batch 128), plus one training step of the network."""
+    from photonfdtd_b200 import surrogate as S
+    peak, kind = bf16_peak()
+    sq = S.gemm_tflops(8192, 8192, 8192, reps=10)
+    layer = S.gemm_tflops(128 * 64, 256, 1152, reps=50)
+    return {"kernel": "k_gemm_tc (tcgen05.mma kind::f16, TMA 128B-swizzle ring, TMEM accumulator)",
+            "roofline": {"bound": "tensor", "achieved": round(sq, 1), "peak": peak,
+                         "unit": "TFLOP/s", "frac": round(sq / peak, 4), "peak_source": kind,
+                         "shape": "8192x8192x8192 bf16 -> f32"},
+            "largest_layer_tflops": round(layer, 1),
+            "largest_layer_shape": "8192x256x1152 (conv4 forward: 3x3 stride 2, 128 -> 256 channels, 8x8 output, batch 128)",
+            "train_step_ms": round(S.time_training_step(128, 20), 3), "train_batch": 128}
 
 
 def traffic_record(kernel_kind):
@@ -416,6 +443,8 @@ def main():
             adj["value"] = round(float(tt.item()), 3)
             adj["scaling"] = "weak (one batch per rank)"
         line["adjoint"] = adj
+    if rank == 0 and world == 1 and not args.no_surrogate:
+        line["surrogate"] = surrogate_bench()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.size)
     if dist is not None:

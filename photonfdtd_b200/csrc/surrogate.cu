@@ -455,6 +455,81 @@ __global__ void k_col2im(int nb, int H, int W, int C, int kh, int kw, int stride
   }
 }
 
+// Vector forms of the two lowerings (32-bit indices; the host checks the
+// sizes and 16-byte alignment). im2col: one thread per 8-column chunk of a
+// col row (one 16-byte store); when C % 8 == 0 a chunk is 8 channels of one
+// tap, read with one 16-byte load. col2im: one thread per 8 channels of an
+// input position (C % 8 == 0), the taps summed in the same order as k_col2im,
+// so both forms give identical results.
+template <bool VEC>
+__global__ void k_im2col8(int rows, int H, int W, int C, int kh, int kw, int stride, int ph,
+                          int pw, int Ho, int Wo, const __nv_bfloat16* x, __nv_bfloat16* col,
+                          int Kp) {
+  const int qn = Kp >> 3, K = kh * kw * C;
+  const int total = rows * qn;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int q = t % qn, m = t / qn;
+    const int ox = m % Wo, r = m / Wo, oy = r % Ho, b = r / Ho;
+    const int k0 = q * 8;
+    uint4 out = make_uint4(0, 0, 0, 0);
+    if (VEC) {
+      if (k0 < K) {
+        const int tap = k0 / C, c = k0 - tap * C, kx = tap % kw, ky = tap / kw;
+        const int iy = oy * stride - ph + ky, ix = ox * stride - pw + kx;
+        if (iy >= 0 && iy < H && ix >= 0 && ix < W)
+          out = *reinterpret_cast<const uint4*>(x + ((long long)(b * H + iy) * W + ix) * C + c);
+      }
+    } else {
+      __nv_bfloat16 v[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        v[e] = __float2bfloat16(0.f);
+        const int k = k0 + e;
+        if (k < K) {
+          const int c = k % C, tap = k / C, kx = tap % kw, ky = tap / kw;
+          const int iy = oy * stride - ph + ky, ix = ox * stride - pw + kx;
+          if (iy >= 0 && iy < H && ix >= 0 && ix < W)
+            v[e] = x[((long long)(b * H + iy) * W + ix) * C + c];
+        }
+      }
+      out = *reinterpret_cast<const uint4*>(v);
+    }
+    *reinterpret_cast<uint4*>(col + (long long)m * Kp + k0) = out;
+  }
+}
+
+__global__ void k_col2im8(int nb, int H, int W, int C, int kh, int kw, int stride, int ph, int pw,
+                          int Ho, int Wo, const float* dcol, int Kp, float* dx) {
+  const int cg = C >> 3;
+  const int total = nb * H * W * cg;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int g = t % cg, p = t / cg;
+    const int ix = p % W, r = p / W, iy = r % H, b = r / H;
+    const int c0 = g * 8;
+    float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0;
+    for (int ky = 0; ky < kh; ++ky) {
+      const int ny = iy + ph - ky;
+      if (ny < 0 || ny % stride) continue;
+      const int oy = ny / stride;
+      if (oy >= Ho) continue;
+      for (int kx = 0; kx < kw; ++kx) {
+        const int nx = ix + pw - kx;
+        if (nx < 0 || nx % stride) continue;
+        const int ox = nx / stride;
+        if (ox >= Wo) continue;
+        const float4* src = reinterpret_cast<const float4*>(
+            dcol + (long long)((b * Ho + oy) * Wo + ox) * Kp + (ky * kw + kx) * C + c0);
+        const float4 u = src[0], v = src[1];
+        s0.x += u.x; s0.y += u.y; s0.z += u.z; s0.w += u.w;
+        s1.x += v.x; s1.y += v.y; s1.z += v.z; s1.w += v.w;
+      }
+    }
+    float4* dst = reinterpret_cast<float4*>(dx + (long long)p * C + c0);
+    dst[0] = s0;
+    dst[1] = s1;
+  }
+}
+
 // y = act(x + bias) over an M x N row-major matrix; FP32 and BF16 outputs
 // (either may be NULL).
 __global__ void k_bias_act(long long M, int N, const float* x, const float* bias, int relu,
@@ -785,9 +860,21 @@ int pfs_im2col(int nb, int H, int W, int C, int kh, int kw, int stride, int ph, 
   const int Ho = (H + 2 * ph - kh) / stride + 1, Wo = (W + 2 * pw - kw) / stride + 1;
   if (Ho < 1 || Wo < 1) return sfail(PF_ERR_INVALID, "pfs_im2col: empty output");
   const long long n = (long long)nb * Ho * Wo * Kp;
-  k_im2col<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(
-      nb, H, W, C, kh, kw, stride, ph, pw, Ho, Wo, (const __nv_bfloat16*)x, (__nv_bfloat16*)col,
-      Kp);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (Kp % 8 == 0 && n / 8 < (1LL << 31) && aligned16(col)) {
+    const int rows = nb * Ho * Wo;
+    if (C % 8 == 0 && aligned16(x))
+      k_im2col8<true><<<grid_for(n / 8, 256), 256, 0, st>>>(rows, H, W, C, kh, kw, stride, ph, pw,
+                                                           Ho, Wo, (const __nv_bfloat16*)x,
+                                                           (__nv_bfloat16*)col, Kp);
+    else
+      k_im2col8<false><<<grid_for(n / 8, 256), 256, 0, st>>>(rows, H, W, C, kh, kw, stride, ph,
+                                                            pw, Ho, Wo, (const __nv_bfloat16*)x,
+                                                            (__nv_bfloat16*)col, Kp);
+  } else {
+    k_im2col<<<grid_for(n, 256), 256, 0, st>>>(nb, H, W, C, kh, kw, stride, ph, pw, Ho, Wo,
+                                               (const __nv_bfloat16*)x, (__nv_bfloat16*)col, Kp);
+  }
   return cuda_status("pfs_im2col");
 }
 
@@ -799,8 +886,14 @@ int pfs_col2im(int nb, int H, int W, int C, int kh, int kw, int stride, int ph, 
   const int Ho = (H + 2 * ph - kh) / stride + 1, Wo = (W + 2 * pw - kw) / stride + 1;
   if (Ho < 1 || Wo < 1) return sfail(PF_ERR_INVALID, "pfs_col2im: empty output");
   const long long n = (long long)nb * H * W * C;
-  k_col2im<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(nb, H, W, C, kh, kw, stride, ph,
-                                                               pw, Ho, Wo, dcol, Kp, dx);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (C % 8 == 0 && Kp % 4 == 0 && n < (1LL << 31) && (long long)nb * Ho * Wo * Kp < (1LL << 31) &&
+      aligned16(dcol) && aligned16(dx))
+    k_col2im8<<<grid_for(n / 8, 256), 256, 0, st>>>(nb, H, W, C, kh, kw, stride, ph, pw, Ho, Wo,
+                                                    dcol, Kp, dx);
+  else
+    k_col2im<<<grid_for(n, 256), 256, 0, st>>>(nb, H, W, C, kh, kw, stride, ph, pw, Ho, Wo, dcol,
+                                               Kp, dx);
   return cuda_status("pfs_col2im");
 }
 

@@ -433,6 +433,57 @@ class SurrogateNet:
 # --------------------------------------------------------------------------- #
 # Spectra from the FDTD engine
 # --------------------------------------------------------------------------- #
+def time_training_step(batch: int = 128, steps: int = 20, warmup: int = 3) -> float:
+    """Milliseconds per training step (forward, loss, backward, AdamW) of the
+    network on random inputs, by CUDA events after `warmup` steps."""
+    import torch
+    net = SurrogateNet(batch)
+    x = torch.rand(batch, 64, 64, device="cuda") * 2 - 1
+    t = torch.randn(batch, N_FREQ, 2, device="cuda")
+
+    def step():
+        net.forward(x)
+        net.loss_grad(t)
+        net.backward()
+        net.adam_step(1e-3)
+    for _ in range(warmup):
+        step()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def gemm_tflops(m: int, n: int, k: int, reps: int = 10, warmup: int = 3) -> float:
+    """TFLOP/s (2mnk per call) of pfs_gemm_bf16 on random BF16 operands,
+    C = A B^T with A m x k and B n x k, timed by CUDA events on the current
+    stream after `warmup` calls."""
+    import torch
+    L = N.lib()
+    st = torch.cuda.current_stream().cuda_stream
+    A = torch.randn(m, k, device="cuda").to(torch.bfloat16)
+    B = torch.randn(n, k, device="cuda").to(torch.bfloat16)
+    Cm = torch.empty(m, n, device="cuda")
+
+    def run():
+        rc = L.pfs_gemm_bf16(m, n, k, A.data_ptr(), k, B.data_ptr(), k, Cm.data_ptr(), n, 1.0,
+                             0.0, st)
+        if rc != N.PF_OK:
+            raise N.NativeError(rc, L.pfs_last_error().decode())
+    for _ in range(warmup):
+        run()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        run()
+    e1.record()
+    torch.cuda.synchronize()
+    return 2.0 * m * n * k / (e0.elapsed_time(e1) / reps) / 1e9
+
+
 class SpectrumGenerator:
     """Transmission spectra of the config-5 geometry for many designs, from
     one forward-only FDTD batch of `batch` copies of the geometry (designs

@@ -45,6 +45,9 @@ def main(argv=None):
                    help="only time this many training steps on random inputs (batch --batch)")
     p.add_argument("--gemm-engine", type=int, default=1, choices=(0, 1),
                    help="tensor-core GEMM engine: 1 tcgen05 (default), 0 mma.sync")
+    p.add_argument("--gemm-shape", default=None,
+                   help="M,N,K: only time pfs_gemm_bf16 at this shape (--reps calls)")
+    p.add_argument("--reps", type=int, default=10)
     p.add_argument("--data", default=None,
                    help="npz of cached spectra (T_train, T_heldout); written if absent")
     a = p.parse_args(argv)
@@ -54,39 +57,18 @@ def main(argv=None):
     rep = {}
     from . import _native as N
     N.lib().pfs_gemm_engine(a.gemm_engine)
+    if a.gemm_shape:
+        M, Nn, K = (int(v) for v in a.gemm_shape.split(","))
+        print(json.dumps({"gemm_engine": a.gemm_engine, "shape": [M, Nn, K],
+                          "tflops": round(S.gemm_tflops(M, Nn, K, reps=a.reps), 1)}))
+        return
     if a.profile_steps:
-        net = S.SurrogateNet(a.batch)
-        x = torch.rand(a.batch, 64, 64, device="cuda") * 2 - 1
-        t = torch.randn(a.batch, 32, 2, device="cuda")
-        for _ in range(3):
-            net.forward(x); net.loss_grad(t); net.backward(); net.adam_step(1e-3)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(a.profile_steps):
-            net.forward(x); net.loss_grad(t); net.backward(); net.adam_step(1e-3)
-        e1.record()
-        torch.cuda.synchronize()
         out = {"batch": a.batch, "gemm_engine": a.gemm_engine,
-               "train_step_ms": e0.elapsed_time(e1) / a.profile_steps}
+               "train_step_ms": S.time_training_step(a.batch, a.profile_steps)}
         # the GEMM kernel alone: a square case and the largest forward layers
-        L = N.lib()
-        st = torch.cuda.current_stream().cuda_stream
         for (M, Nn, K) in [(8192, 8192, 8192), (a.batch * 64, 256, 1152),
                            (a.batch * 16, 128, 2304)]:
-            A = torch.randn(M, K, device="cuda").to(torch.bfloat16)
-            B = torch.randn(Nn, K, device="cuda").to(torch.bfloat16)
-            Cm = torch.empty(M, Nn, device="cuda")
-            run = lambda: L.pfs_gemm_bf16(M, Nn, K, A.data_ptr(), K, B.data_ptr(), K,
-                                          Cm.data_ptr(), Nn, 1.0, 0.0, st)
-            for _ in range(3):
-                run()
-            e0.record()
-            for _ in range(10):
-                run()
-            e1.record()
-            torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1) / 10
-            out[f"gemm_{M}x{Nn}x{K}_tflops"] = round(2 * M * Nn * K / ms / 1e9, 1)
+            out[f"gemm_{M}x{Nn}x{K}_tflops"] = round(S.gemm_tflops(M, Nn, K), 1)
         print(json.dumps(out))
         return
 
