@@ -61,6 +61,8 @@ def parse():
     p.add_argument("--size", type=int, default=384, help="cells per axis (default 384)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-reference-gpu", action="store_true",
+                   help="skip timing the reference's own CUDA kernels on the plain variant")
     p.add_argument("--no-surrogate", action="store_true",
                    help="skip the surrogate tensor-core GEMM / training-step figures")
     p.add_argument("--no-adjoint", action="store_true")
@@ -204,6 +206,54 @@ def surrogate_bench():
             "largest_layer_tflops": round(layer, 1),
             "largest_layer_shape": "8192x256x1152 (conv4 forward: 3x3 stride 2, 128 -> 256 channels, 8x8 output, batch 128)",
             "train_step_ms": round(S.time_training_step(128, 20), 3), "train_batch": 128}
+
+
+def reference_gpu_bench(size: int, steps: int = 100, warmup: int = 5):
+    """The reference's own CUDA stepping kernels (rust/src/cuda.rs:29-265,
+    compiled for sm_100a by baseline/refcuda/build.py) against this engine on
+    the workload they can both run: the config-3 grid and media blocks with
+    non-dispersive media (eps 1.0 / 4.0 / 2.1), float32, no monitors. Both
+    timed by CUDA events on their own streams; `agreement` is the relative L2
+    difference of the final Ex."""
+    import torch
+    from baseline import refcuda
+    if not refcuda.available("float32"):
+        return {"unavailable": "baseline/_ref/librefcuda_f32.so not built"}
+    import photonfdtd_b200 as pf
+    from photonfdtd_b200 import workloads as W
+    from photonfdtd_b200.engine import B200Engine, build_tables
+    sim = W.config3(pf, n_total=size, n_steps=warmup + steps, flux=False, dft=False,
+                    dispersive=False)
+    cells = size ** 3
+    eng = B200Engine(build_tables(sim))
+    st = torch.cuda.ExternalStream(eng.stream())
+    eng.advance(0, warmup)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    eng.advance(warmup, steps)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ours_ms = e0.elapsed_time(e1)
+    ex = eng.get("Ex").astype(np.float64)
+    eng.close()
+    ref = refcuda.RefCuda(sim)
+    try:
+        ref.run(0, warmup)
+        ref_ms = ref.run(warmup, steps, timed=True)
+        rx = ref.field("Ex").astype(np.float64)
+    finally:
+        ref.close()
+    return {"workload": f"config3 grid {size}^3, media eps 1.0/4.0/2.1 in 8^3 blocks "
+                        "(no ADE), Yee+CPML float32, Ex dipole, no monitors",
+            "steps": steps, "unit": "Mcell-updates/s",
+            "reference_kernels": round(cells * steps / (ref_ms / 1e3) / 1e6, 1),
+            "reference_kernels_ms_per_step": round(ref_ms / steps, 4),
+            "b200_engine": round(cells * steps / (ours_ms / 1e3) / 1e6, 1),
+            "b200_engine_ms_per_step": round(ours_ms / steps, 4),
+            "agreement_ex_rel_l2": float(np.linalg.norm(ex - rx) / np.linalg.norm(rx)),
+            "source": "reference rust/src/cuda.rs update_h / update_e / inject, nvcc "
+                      "sm_100a, launched as Inner::run_steps (1024-thread blocks)"}
 
 
 def traffic_record(kernel_kind):
@@ -443,6 +493,8 @@ def main():
             adj["value"] = round(float(tt.item()), 3)
             adj["scaling"] = "weak (one batch per rank)"
         line["adjoint"] = adj
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        line["reference_gpu"] = reference_gpu_bench(args.size)
     if rank == 0 and world == 1 and not args.no_surrogate:
         line["surrogate"] = surrogate_bench()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -104,13 +104,20 @@ def config3_block_ids(n_blocks: int, seed: int = 3) -> np.ndarray:
     return np.random.default_rng(seed).integers(0, 3, size=(n_blocks,) * 3)
 
 
+def config3_plain_media(pf):
+    """Non-dispersive stand-ins for the three media (eps 1.0 / 4.0 / 2.1): the
+    workload the reference's CUDA kernels can run (scalar ce, no ADE)."""
+    return tuple(pf.Medium(permittivity=e) for e in (1.0, 4.0, 2.1))
+
+
 def config3(pf, n_total: int = 384, block: int = 8, n_steps: int = 3000,
             flux: bool = True, dft: bool = True, precision: str = "float32",
-            flux_pos: float = None):
-    """3D dispersive ADE mix in 8^3 blocks, six flux planes, a z-plane DFT."""
+            flux_pos: float = None, dispersive: bool = True):
+    """3D dispersive ADE mix in 8^3 blocks, six flux planes, a z-plane DFT.
+    dispersive=False swaps in config3_plain_media (same grid and blocks)."""
     d = 10e-9
     grid = pf.Grid(size=(n_total * d,) * 3, cell_size=d, pml_layers=12)
-    media = config3_media(pf)
+    media = config3_media(pf) if dispersive else config3_plain_media(pf)
     nb = n_total // block
     ids = config3_block_ids(nb)
     x0 = -(n_total - 1) / 2 * d            # coordinate of cell 0
