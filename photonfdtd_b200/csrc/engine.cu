@@ -11,6 +11,7 @@
 //   monitors sample rings + complex128 accumulators (DFT), block partials +
 //            float64 accumulators (flux)
 #include <algorithm>
+#include <type_traits>
 #include <cstdarg>
 #include <cstdio>
 #include <cmath>
@@ -494,6 +495,18 @@ StepArgs<T> step_args(pf_engine* e) {
 }
 
 template <typename T>
+void launch_h_split(pf_engine* e, const StepArgs<T>& a, dim3 g, dim3 b) {
+  if constexpr (std::is_same<T, float>::value) {
+    if (PFB_H_ROWS == 2 && b.x == 32 && b.y == 8) {  // 3D: two rows per thread, packed
+      g.y = (e->ny + 15) / 16;
+      k_h_split2<<<g, b, 0, e->stream>>>(a);
+      return;
+    }
+  }
+  k_h_split<T><<<g, b, 0, e->stream>>>(a);
+}
+
+template <typename T>
 void launch_e_split(pf_engine* e, const StepArgs<T>& a, dim3 g, dim3 b) {
   const bool ade = e->n_media > 0;
   switch (e->ce_mode) {
@@ -609,7 +622,7 @@ int advance_typed(pf_engine* e, long long n_sub) {
     } else {
       {
         LaunchScope ls(e, 0);
-        k_h_split<T><<<grd, blk, 0, e->stream>>>(a);
+        launch_h_split<T>(e, a, grd, blk);
       }
       inject<T>(e, 1, nxt, s);
       a.Hin[0] = a.Hout[0];

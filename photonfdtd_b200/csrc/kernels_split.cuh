@@ -17,6 +17,7 @@
 #pragma once
 
 #include "cell3d.cuh"
+#include "packed2.cuh"
 
 // Minimum resident 256-thread blocks per SM the split passes are compiled
 // for (register budget 65536 / (256 * n)). Measured on config 3 (384^3 ADE):
@@ -28,6 +29,13 @@
 #endif
 #ifndef PFB_MINB_E
 #define PFB_MINB_E 5
+#endif
+// Two-row packed H pass (k_h_split2) for float32 3D grids: 1 enables it.
+#ifndef PFB_H_ROWS
+#define PFB_H_ROWS 2
+#endif
+#ifndef PFB_MINB_H2
+#define PFB_MINB_H2 6
 #endif
 
 namespace pfb {
@@ -66,15 +74,10 @@ __device__ __forceinline__ bool in_box(int i, int j0, int j1, int k0, int k1, co
   return i >= b0[0] && i < b1[0] && j0 >= b0[1] && j1 <= b1[1] && k0 >= b0[2] && k1 <= b1[2];
 }
 
-// H pass: H^{n+1/2} = H^{n-1/2} - ch (curl E^n + psi).
+// H pass: H^{n+1/2} = H^{n-1/2} - ch (curl E^n + psi). One cell; `box`:
+// the cell's block lies in the bulk box.
 template <typename T>
-__global__ void __launch_bounds__(256, PFB_MINB_H) k_h_split(const __grid_constant__ StepArgs<T> a) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int i = blockIdx.z;
-  const bool box = in_box(i, blockIdx.y * blockDim.y, (blockIdx.y + 1) * blockDim.y,
-                          blockIdx.x * blockDim.x, (blockIdx.x + 1) * blockDim.x, a.hb0, a.hb1);
-  if (k >= a.nz || j >= a.ny) return;
+__device__ __forceinline__ void h_cell(const StepArgs<T>& a, int i, int j, int k, bool box) {
   const long long sy = a.nz, sx = (long long)a.ny * a.nz;
   const long long id = i * sx + j * sy + k;
   const T ex = a.Ein[0][id], ey = a.Ein[1][id], ez = a.Ein[2][id];
@@ -113,6 +116,82 @@ __global__ void __launch_bounds__(256, PFB_MINB_H) k_h_split(const __grid_consta
                             ld_if(a.Ein[2], id, sx, hx), ez, true);
   a.Hout[2][id] = upd_hz<T>(a, i, j, k, a.Hin[2][id], ld_if(a.Ein[1], id, sx, hx), ey,
                             ld_if(a.Ein[0], id, sy, hy), ex, true);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, PFB_MINB_H) k_h_split(const __grid_constant__ StepArgs<T> a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  const bool box = in_box(i, blockIdx.y * blockDim.y, (blockIdx.y + 1) * blockDim.y,
+                          blockIdx.x * blockDim.x, (blockIdx.x + 1) * blockDim.x, a.hb0, a.hb1);
+  if (k >= a.nz || j >= a.ny) return;
+  h_cell<T>(a, i, j, k, box);
+}
+
+// The H pass of 3D float32 grids with two adjacent rows (j, j+1) per thread:
+// a 32 x 8 block covers 32 x 16 cells. In the bulk box the two cells' values
+// travel as float2 pairs through the packed FP32 instructions (packed2.cuh),
+// which round each cell as the scalar path does; row j reuses row j+1's own
+// Ez and Ex as its +y neighbours. Elsewhere (and when a numerator leaves the
+// fast division's range) each cell takes the scalar path.
+__global__ void __launch_bounds__(256, PFB_MINB_H2) k_h_split2(const __grid_constant__ StepArgs<float> a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j0 = (blockIdx.y * blockDim.y + threadIdx.y) * 2;
+  const int i = blockIdx.z;
+  const bool box = in_box(i, blockIdx.y * blockDim.y * 2, (blockIdx.y + 1) * blockDim.y * 2,
+                          blockIdx.x * blockDim.x, (blockIdx.x + 1) * blockDim.x, a.hb0, a.hb1);
+  if (k >= a.nz || j0 >= a.ny) return;
+  if (!box) {
+    h_cell<float>(a, i, j0, k, false);
+    if (j0 + 1 < a.ny) h_cell<float>(a, i, j0 + 1, k, false);
+    return;
+  }
+  const long long sy = a.nz, sx = (long long)a.ny * a.nz;
+  const long long id0 = i * sx + j0 * sy + k, id1 = id0 + sy;
+  const float2 ex = make_float2(a.Ein[0][id0], a.Ein[0][id1]);
+  const float2 ey = make_float2(a.Ein[1][id0], a.Ein[1][id1]);
+  const float2 ez = make_float2(a.Ein[2][id0], a.Ein[2][id1]);
+  const float2 f0 = make_float2(a.Hin[0][id0], a.Hin[0][id1]);
+  const float2 f1 = make_float2(a.Hin[1][id0], a.Hin[1][id1]);
+  const float2 f2 = make_float2(a.Hin[2][id0], a.Hin[2][id1]);
+  // Hx: +dEz/dy - dEy/dz; Hy: +dEx/dz - dEz/dx; Hz: +dEy/dx - dEx/dy
+  const float2 n0 = sub2(make_float2(ez.y, a.Ein[2][id1 + sy]), ez);
+  const float2 n1 = sub2(make_float2(a.Ein[1][id0 + 1], a.Ein[1][id1 + 1]), ey);
+  const float2 n2 = sub2(make_float2(a.Ein[0][id0 + 1], a.Ein[0][id1 + 1]), ex);
+  const float2 n3 = sub2(make_float2(a.Ein[2][id0 + sx], a.Ein[2][id1 + sx]), ez);
+  const float2 n4 = sub2(make_float2(a.Ein[1][id0 + sx], a.Ein[1][id1 + sx]), ey);
+  const float2 n5 = sub2(make_float2(ex.y, a.Ein[0][id1 + sy]), ex);
+  const float m = fmaxf(fmaxf(absmax2(n0, n1), absmax2(n2, n3)), absmax2(n4, n5));
+  if (!(a.fdx && a.fdy && a.fdz && qdiv_ok(m))) {
+    // a numerator outside the fast division's range: the scalar path
+    const float nn[2][6] = {{n0.x, n1.x, n2.x, n3.x, n4.x, n5.x},
+                            {n0.y, n1.y, n2.y, n3.y, n4.y, n5.y}};
+    const float ff[2][3] = {{f0.x, f1.x, f2.x}, {f0.y, f1.y, f2.y}};
+    const float mch = -a.ch;
+    const float K[3] = {mch, mch, mch};
+    const int ax[6] = {1, 2, 2, 0, 0, 1};
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      float h[3];
+      bulk3<float>(a, ff[r], K, nn[r], ax, h);
+      const long long id = r ? id1 : id0;
+      a.Hout[0][id] = h[0];
+      a.Hout[1][id] = h[1];
+      a.Hout[2][id] = h[2];
+    }
+    return;
+  }
+  const float2 K = bc2(-a.ch);
+  const float2 h0 = bulk2(f0, K, qdiv_fast2(n0, a.dy, a.rdy), qdiv_fast2(n1, a.dz, a.rdz));
+  const float2 h1 = bulk2(f1, K, qdiv_fast2(n2, a.dz, a.rdz), qdiv_fast2(n3, a.dx, a.rdx));
+  const float2 h2 = bulk2(f2, K, qdiv_fast2(n4, a.dx, a.rdx), qdiv_fast2(n5, a.dy, a.rdy));
+  a.Hout[0][id0] = h0.x;
+  a.Hout[0][id1] = h0.y;
+  a.Hout[1][id0] = h1.x;
+  a.Hout[1][id1] = h1.y;
+  a.Hout[2][id0] = h2.x;
+  a.Hout[2][id1] = h2.y;
 }
 
 // E pass: E^{n+1} = E^n + ce (curl H^{n+1/2} + psi), then ADE.
