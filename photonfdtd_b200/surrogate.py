@@ -757,6 +757,35 @@ def _sync():
     torch.cuda.synchronize()
 
 
+def trajectory_data(problem: FDTDDesignProblem, param: SmoothDesign, seeds: Sequence[int],
+                    iters: int, lr: float = 0.05, every: int = 1,
+                    log: Optional[Callable] = None) -> Tuple[np.ndarray, np.ndarray]:
+    """Training pairs from optimisation trajectories: the plain adjoint loop
+    (plain_adjoint_loop's steps) run on problem.n designs at a time from the
+    latent starts of `seeds`; every `every`-th iterate's density and its
+    float32 FDTD spectrum (the forward pass of that iteration's gradient, so
+    no extra FDTD run) are recorded. Returns (rho, T) stacked in the order
+    [chunk of problem.n designs][recorded iteration][design]."""
+    B = problem.n
+    rhos, Ts = [], []
+    for c0 in range(0, len(seeds) - B + 1, B):
+        z = param.start(list(seeds[c0:c0 + B]))
+        opt = _Adam(z.shape, lr)
+        t0 = time.perf_counter()
+        v = np.zeros(B)
+        for it in range(iters):
+            rho = param.rho(z)
+            v, g, T = problem.value_grad_spectra(rho)
+            if it % every == 0:
+                rhos.append(rho.astype(np.float32))
+                Ts.append(T)
+            z = opt.ascend(z, param.grad_z(z, g))
+        if log is not None:
+            log(f"trajectories {c0}-{c0 + B - 1}: {iters} iterations in "
+                f"{time.perf_counter() - t0:.1f} s, final objective {float(np.mean(v)):.4f}")
+    return np.concatenate(rhos), np.concatenate(Ts)
+
+
 def plain_adjoint_loop(problem: FDTDDesignProblem, param: SmoothDesign, z0: np.ndarray,
                        iters: int = 200, lr: float = 0.05) -> Dict:
     """Gradient ascent on the latent design z with the FDTD adjoint gradient
@@ -780,81 +809,107 @@ def plain_adjoint_loop(problem: FDTDDesignProblem, param: SmoothDesign, z0: np.n
 def surrogate_loop(problem: FDTDDesignProblem, net: SurrogateNet, param: SmoothDesign,
                    z0: np.ndarray, iters: int = 200, lr: float = 0.05,
                    verify_every: int = 10, max_error: float = 0.02,
-                   tuner: Optional[OnlineTuner] = None, target: Optional[float] = None) -> Dict:
-    """Gradient ascent on z in bursts of `verify_every` iterations, each
-    burst using surrogate gradients or, in fallback, the FDTD adjoint
-    gradient. After every burst the FDTD forward run verifies the designs:
-      * fallback for the next burst when the surrogate's power-transmission
-        error (power_error, mean over the designs) exceeds `max_error`;
-      * a surrogate burst that did not raise the verified objective is
-        rolled back, its step size halved (a trust region), and the next
-        burst runs in fallback; an accepted burst restores the step size;
-      * every FDTD spectrum computed feeds `tuner` (online fine-tuning).
-    With `target`, records the wall-clock at which the verified objective
-    first reaches target - 1 % |target|."""
+                   tuner: Optional[OnlineTuner] = None, target: Optional[float] = None,
+                   fallback_steps: int = 3, max_tries: int = 3, burst_lr: Optional[float] = None,
+                   max_bursts: int = 1) -> Dict:
+    """Surrogate-assisted gradient ascent on z with first-order model
+    management (the additive-correction trust-region scheme of Alexandrov,
+    Dennis, Lewis and Torczon, 1998). Each cycle:
+      1. one plain step with the FDTD adjoint gradient g at the current
+         design, whose forward pass also gives the verified objective there;
+         the surrogate's gradient at the same design gives the correction
+         d = g - g_sur, so the corrected model g_sur + d is exact to first
+         order at that design;
+      2. bursts of `verify_every` Adam steps on the corrected surrogate
+         gradient (step size burst_lr, default lr), each verified by the FDTD
+         forward run: a burst that raised the verified objective is kept and
+         the next one follows (at most `max_bursts` kept per cycle); one that
+         did not is rolled back (design and Adam state) and retried with half
+         the step, at most `max_tries` rejections per cycle;
+      3. fallback: when the surrogate's power-transmission error on the last
+         verified design (power_error, mean over the designs) exceeds
+         `max_error`, the next cycle takes `fallback_steps` plain FDTD steps
+         before its bursts.
+    Every FDTD spectrum feeds `tuner` (online fine-tuning). Iterations are
+    design updates: FDTD steps and kept surrogate steps count toward `iters`,
+    rolled-back bursts do not. With `target`, records the wall-clock at which
+    the best verified objective first reaches target - 1 % |target|."""
     z = np.array(z0, np.float64)
     opt = _Adam(z.shape, lr)
-    v0, T0 = problem.value(param.rho(z))
-    best_z, best_v, best_opt = z.copy(), float(np.mean(v0)), None
-    if tuner is not None:
-        tuner.add(param.rho(z), T0)
-        tuner.tune()
-    step = lr
-    fallback = 0
+    blr = lr if burst_lr is None else burst_lr
+    best_z, best_v = z.copy(), -np.inf
     log = []
-    n_fdtd_grad, n_verify, n_reject = 0, 1, 0
+    n_fdtd_grad, n_verify, n_reject, n_kept = 0, 0, 0, 0
     reached = None
+    n_plain = 1
     _sync()
     t0 = time.perf_counter()
     it = 0
+
+    def note(v, zz):
+        nonlocal best_v, best_z, reached
+        if v > best_v:
+            best_v, best_z = v, zz.copy()
+        if target is not None and reached is None and best_v >= target - 0.01 * abs(target):
+            reached = time.perf_counter() - t0
+
     while it < iters:
-        use_fdtd = fallback > 0
-        opt.lr = lr if use_fdtd else step
-        saved = (opt.m.copy(), opt.v.copy(), opt.t)
-        for _ in range(min(verify_every, iters - it)):
+        # 1. plain FDTD steps; the last one's gradient corrects the surrogate
+        for _ in range(min(n_plain, iters - it)):
             rho = param.rho(z)
-            if use_fdtd:
-                _, g, T = problem.value_grad_spectra(rho)
-                n_fdtd_grad += 1
-                if tuner is not None:
-                    tuner.add(rho, T)
-            else:
-                _, g = net.value_and_grad(rho, band_objective)
+            v, g, T = problem.value_grad_spectra(rho)
+            n_fdtd_grad += 1
+            cur_v = float(np.mean(v))
+            note(cur_v, z)
+            if tuner is not None:
+                tuner.add(rho, T)
+            _, g_sur = net.value_and_grad(rho, band_objective)
+            delta = g - g_sur
+            opt.lr = lr
             z = opt.ascend(z, param.grad_z(z, g))
             it += 1
-        fallback = 0
-        rho = param.rho(z)
-        v_true, T_true = problem.value(rho)
-        n_verify += 1
-        vt = float(np.mean(v_true))
-        T_sur = net.predict(rho)
-        perr = float(np.mean(power_error(T_sur, T_true)))
-        cerr = float(np.mean(np.linalg.norm(T_sur - T_true, axis=1) /
-                             np.linalg.norm(T_true, axis=1)))
-        accepted = use_fdtd or vt > best_v
-        if accepted:
-            best_z, best_v = z.copy(), max(best_v, vt) if not use_fdtd else vt
-            if not use_fdtd:
-                step = lr
-        else:  # roll the surrogate burst back, shrink its step, let FDTD take the next one
-            z = best_z.copy()
-            opt.m, opt.v, opt.t = saved
-            step *= 0.5
-            n_reject += 1
-            fallback = verify_every
-        if perr > max_error:
-            fallback = verify_every
-        now = time.perf_counter() - t0
-        log.append({"iter": it, "t": round(now, 3), "objective": vt, "source":
-                    "fdtd" if use_fdtd else "surrogate", "accepted": bool(accepted),
-                    "power_error": perr, "complex_error": cerr})
-        if target is not None and reached is None and best_v >= target - 0.01 * abs(target):
-            reached = now
+        if it >= iters:
+            break
+        # 2. corrected surrogate bursts, each verified
+        step, kept, rejected, perr, vt = blr, 0, 0, 0.0, cur_v
+        while kept < max_bursts and rejected < max_tries and it < iters:
+            saved = (z.copy(), opt.m.copy(), opt.v.copy(), opt.t)
+            opt.lr = step
+            n = min(verify_every, iters - it)
+            for _ in range(n):
+                _, gs = net.value_and_grad(param.rho(z), band_objective)
+                z = opt.ascend(z, param.grad_z(z, gs + delta))
+            rho = param.rho(z)
+            v_true, T_true = problem.value(rho)
+            n_verify += 1
+            vt = float(np.mean(v_true))
+            if tuner is not None:
+                tuner.add(rho, T_true)
+            perr = float(np.mean(power_error(net.predict(rho), T_true)))
+            if vt > cur_v:
+                cur_v = vt
+                it += n
+                n_kept += n
+                kept += 1
+                note(vt, z)
+            else:
+                z, opt.m, opt.v, opt.t = saved
+                step *= 0.5
+                rejected += 1
+                n_reject += 1
+        # 3. fallback when the surrogate is off by more than max_error
+        n_plain = fallback_steps if perr > max_error else 1
+        log.append({"iter": it, "t": round(time.perf_counter() - t0, 3), "best": best_v,
+                    "objective": cur_v, "bursts_kept": kept, "bursts_rejected": rejected,
+                    "power_error": perr, "next_fdtd_steps": n_plain})
         if tuner is not None:
-            tuner.add(rho, T_true)
             tuner.tune()
+    v_end, _ = problem.value(param.rho(z))
+    n_verify += 1
+    note(float(np.mean(v_end)), z)
     _sync()
     wall = time.perf_counter() - t0
     return {"z": best_z, "final": best_v, "wall_s": wall, "log": log,
             "fdtd_gradients": n_fdtd_grad, "fdtd_verifications": n_verify,
-            "surrogate_bursts_rejected": n_reject, "reached_target_s": reached}
+            "surrogate_steps_kept": n_kept, "surrogate_bursts_rejected": n_reject,
+            "reached_target_s": reached}

@@ -48,6 +48,17 @@ def main(argv=None):
     p.add_argument("--gemm-shape", default=None,
                    help="M,N,K: only time pfs_gemm_bf16 at this shape (--reps calls)")
     p.add_argument("--reps", type=int, default=10)
+    p.add_argument("--traj-designs", type=int, default=0,
+                   help="add training pairs from plain adjoint trajectories of this many "
+                        "designs (latent seeds 100000+)")
+    p.add_argument("--traj-batch", type=int, default=64)
+    p.add_argument("--traj-iters", type=int, default=100)
+    p.add_argument("--traj-every", type=int, default=2)
+    p.add_argument("--traj-heldout", type=int, default=0,
+                   help="of the trajectory designs, this many (the last whole batches) are "
+                        "held out for evaluation")
+    p.add_argument("--loop-variants", default="3:1:1",
+                   help="surrogate loops to run, comma-separated FALLBACK:BURST_LR_MULT:MAX_BURSTS")
     p.add_argument("--data", default=None,
                    help="npz of cached spectra (T_train, T_heldout); written if absent")
     a = p.parse_args(argv)
@@ -104,6 +115,26 @@ def main(argv=None):
                        "heldout_gcell_per_s_f64": round(ch / wh / 1e9, 1)}
         if a.data:
             np.savez_compressed(a.data, T_train=T_t, T_heldout=T_h)
+    rho_jh = T_jh = None
+    if a.traj_designs:
+        B = a.traj_batch
+        prob = S.FDTDDesignProblem(B)
+        param = S.SmoothDesign()
+        t0 = time.perf_counter()
+        rj, Tj = S.trajectory_data(prob, param, list(range(100000, 100000 + a.traj_designs)),
+                                   a.traj_iters, every=a.traj_every, log=say)
+        prob.close()
+        per_chunk = len(rj) // (a.traj_designs // B)
+        nh = (a.traj_heldout // B) * per_chunk
+        n_used = len(rj) - nh
+        rho_jh, T_jh = rj[n_used:], Tj[n_used:]
+        rho_t = np.concatenate([rho_t, rj[:n_used].astype(np.float64)])
+        T_t = np.concatenate([T_t, Tj[:n_used]])
+        rep["trajectories"] = {"designs": a.traj_designs, "batch": B, "iters": a.traj_iters,
+                               "every": a.traj_every, "pairs_train": int(n_used),
+                               "pairs_heldout": int(nh), "seeds": "100000+",
+                               "wall_s": round(time.perf_counter() - t0, 1)}
+        say("trajectory data: " + json.dumps(rep["trajectories"]))
     x = tg = None
     if a.weights is None:
         dev = "cuda"
@@ -135,6 +166,13 @@ def main(argv=None):
                                          "p95": float(np.percentile(pe, 95)),
                                          "frac_below_2pct": float(np.mean(pe < 0.02))}
     say("held-out error: " + json.dumps(rep["heldout_error_vs_f64"]))
+    if rho_jh is not None and len(rho_jh):
+        pj = net.predict(rho_jh.astype(np.float64))
+        rep["trajectory_heldout_error_vs_f32"] = S.spectrum_errors(pj, T_jh)
+        pe = S.power_error(pj, T_jh)
+        rep["trajectory_heldout_power_error"] = {"mean": float(pe.mean()),
+                                                 "p95": float(np.percentile(pe, 95))}
+        say("trajectory held-out error: " + json.dumps(rep["trajectory_heldout_error_vs_f32"]))
     say("held-out power error: " + json.dumps(rep["heldout_power_error_vs_f64"]))
 
     if a.loops:
@@ -152,11 +190,22 @@ def main(argv=None):
             x = torch.from_numpy((2.0 * rho_t - 1.0).astype(np.float32)).to("cuda")
             tri = np.stack([T_t.real, T_t.imag], axis=-1)
             tg = torch.from_numpy(((tri - net.t_mean) / net.t_std).astype(np.float32)).to("cuda")
-        tuner = S.OnlineTuner(inf, x, tg)
-        sur = S.surrogate_loop(prob, inf, param, z0, iters=a.loop_iters, tuner=tuner,
-                               target=plain["final"])
-        say(f"surrogate loop: objective {sur['final']:.4f} in {sur['wall_s']:.1f} s, "
-            f"reached plain's objective (1 %) at {sur['reached_target_s']}")
+        params0 = net.params()
+        surs = []
+        for spec in a.loop_variants.split(","):
+            fb, mult, nb = spec.split(":")
+            # every loop starts from the trained network (online tuning changes it)
+            inf = S.SurrogateNet(32, params=params0, t_mean=net.t_mean, t_std=net.t_std)
+            tuner = S.OnlineTuner(inf, x, tg)
+            r = S.surrogate_loop(prob, inf, param, z0, iters=a.loop_iters, tuner=tuner,
+                                 target=plain["final"], fallback_steps=int(fb),
+                                 burst_lr=0.05 * float(mult), max_bursts=int(nb))
+            r["variant"] = {"fallback_steps": int(fb), "burst_lr": 0.05 * float(mult),
+                            "max_bursts": int(nb)}
+            say(f"surrogate loop {spec}: objective {r['final']:.4f} in {r['wall_s']:.1f} s, "
+                f"reached plain's objective (1 %) at {r['reached_target_s']}")
+            surs.append(r)
+        sur = min(surs, key=lambda r: (r["reached_target_s"] or float("inf"), -r["final"]))
         rep["design_loops"] = {
             "designs": nd, "iters": a.loop_iters, "objective": "band_objective",
             "plain": {"final": plain["final"], "wall_s": round(plain["wall_s"], 2),
@@ -167,7 +216,15 @@ def main(argv=None):
                           "fdtd_gradients": sur["fdtd_gradients"],
                           "fdtd_verifications": sur["fdtd_verifications"],
                           "bursts_rejected": sur["surrogate_bursts_rejected"],
-                          "log": sur["log"]},
+                          "surrogate_steps_kept": sur["surrogate_steps_kept"],
+                          "variant": sur["variant"], "log": sur["log"]},
+            "surrogate_variants": [{**r["variant"], "final": r["final"],
+                                    "wall_s": round(r["wall_s"], 2),
+                                    "reached_target_s": r["reached_target_s"],
+                                    "fdtd_gradients": r["fdtd_gradients"],
+                                    "fdtd_verifications": r["fdtd_verifications"],
+                                    "surrogate_steps_kept": r["surrogate_steps_kept"]}
+                                   for r in surs],
             "plain_reached_target_s": plain_reach,
             "speedup_to_target": (round(plain_reach / sur["reached_target_s"], 2)
                                   if sur["reached_target_s"] and plain_reach else None)}
