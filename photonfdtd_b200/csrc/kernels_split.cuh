@@ -19,6 +19,8 @@
 #include "cell3d.cuh"
 #include "packed2.cuh"
 
+#include <type_traits>
+
 // Minimum resident 256-thread blocks per SM the split passes are compiled
 // for (register budget 65536 / (256 * n)). Measured on config 3 (384^3 ADE):
 // H at 8 (32 registers, a 12-byte spill) and E at 5 (48 registers) give
@@ -36,6 +38,10 @@
 #endif
 #ifndef PFB_MINB_H2
 #define PFB_MINB_H2 6
+#endif
+// Packed FP32 pairs inside one cell in the float32 E pass's bulk path.
+#ifndef PFB_E_PAIR
+#define PFB_E_PAIR 1
 #endif
 
 namespace pfb {
@@ -67,6 +73,31 @@ __device__ __forceinline__ void bulk3(const StepArgs<T>& a, const T f[3], const 
   }
 #pragma unroll
   for (int c = 0; c < 3; ++c) out[c] = bulk(f[c], K[c], q[2 * c], q[2 * c + 1]);
+}
+
+// bulk3 for one float32 cell of a 3D grid (divisor axes {1,2,2,0,0,1}) on
+// the packed FP32 instructions: the six divisions as three lane pairs,
+// (n0, n2) by (dy, dz), (n1, n3) by (dz, dx), (n4, n5) by (dx, dy), and the
+// first two components' updates as one pair. Same operations, same order,
+// same fast-path test as bulk3, so the same bits.
+__device__ __forceinline__ void bulk3_pair(const StepArgs<float>& a, const float f[3],
+                                           const float K[3], const float n[6], float out[3]) {
+  const float m = absmax(absmax(n[0], n[1]), absmax(absmax(n[2], n[3]), absmax(n[4], n[5])));
+  if (!(a.fdx && a.fdy && a.fdz && qdiv_ok(m))) {
+    const int ax[6] = {1, 2, 2, 0, 0, 1};
+    bulk3<float>(a, f, K, n, ax, out);
+    return;
+  }
+  const float2 qA = qdiv_fast2v(make_float2(n[0], n[2]), make_float2(a.dy, a.dz),
+                                make_float2(a.rdy, a.rdz));
+  const float2 qB = qdiv_fast2v(make_float2(n[1], n[3]), make_float2(a.dz, a.dx),
+                                make_float2(a.rdz, a.rdx));
+  const float2 qC = qdiv_fast2v(make_float2(n[4], n[5]), make_float2(a.dx, a.dy),
+                                make_float2(a.rdx, a.rdy));
+  const float2 o = bulk2(make_float2(f[0], f[1]), make_float2(K[0], K[1]), qA, qB);
+  out[0] = o.x;
+  out[1] = o.y;
+  out[2] = bulk(f[2], K[2], qC.x, qC.y);
 }
 
 __device__ __forceinline__ bool in_box(int i, int j0, int j1, int k0, int k1, const int* b0,
@@ -240,8 +271,12 @@ __global__ void __launch_bounds__(256, PFB_MINB_E) k_e_split(const __grid_consta
     const T n[6] = {sub_rn(hz, hn[0]), sub_rn(hy, hn[1]), sub_rn(hx, hn[2]),
                     sub_rn(hz, hn[3]), sub_rn(hy, hn[4]), sub_rn(hx, hn[5])};
     if (box) {
-      const int ax[6] = {1, 2, 2, 0, 0, 1};
-      bulk3<T>(a, en, K, n, ax, e);
+      if constexpr (std::is_same<T, float>::value && PFB_E_PAIR) {
+        bulk3_pair(a, en, K, n, e);
+      } else {
+        const int ax[6] = {1, 2, 2, 0, 0, 1};
+        bulk3<T>(a, en, K, n, ax, e);
+      }
     } else {
       e3<T>(a, i, j, k, en, K, n, e);
     }

@@ -28,6 +28,15 @@ __device__ __forceinline__ float2 qdiv_fast2(float2 a, float d, float r) {
   return make_float2(copysignf(q.x, a.x), copysignf(q.y, a.y));
 }
 
+// qdiv_fast2 with a divisor per lane (d.x for a.x, d.y for a.y).
+__device__ __forceinline__ float2 qdiv_fast2v(float2 a, float2 d, float2 r) {
+  const float2 as = mul2(a, bc2(0x1p64f));
+  const float2 q0 = mul2(as, r);
+  const float2 rem = __ffma2_rn(q0, make_float2(-d.x, -d.y), as);
+  const float2 q = mul2(__ffma2_rn(rem, r, q0), bc2(0x1p-64f));
+  return make_float2(copysignf(q.x, a.x), copysignf(q.y, a.y));
+}
+
 // bulk() on two cells: f + (dA - dB) * k.
 __device__ __forceinline__ float2 bulk2(float2 f, float2 k, float2 dA, float2 dB) {
   return add2(f, mul2(sub2(dA, dB), k));
