@@ -810,7 +810,7 @@ def surrogate_loop(problem: FDTDDesignProblem, net: SurrogateNet, param: SmoothD
                    z0: np.ndarray, iters: int = 200, lr: float = 0.05,
                    verify_every: int = 10, max_error: float = 0.02,
                    tuner: Optional[OnlineTuner] = None, target: Optional[float] = None,
-                   fallback_steps: int = 3, max_tries: int = 3, burst_lr: Optional[float] = None,
+                   fallback_steps: int = 1, max_tries: int = 3, burst_lr: Optional[float] = None,
                    max_bursts: int = 1) -> Dict:
     """Surrogate-assisted gradient ascent on z with first-order model
     management (the additive-correction trust-region scheme of Alexandrov,
@@ -826,10 +826,12 @@ def surrogate_loop(problem: FDTDDesignProblem, net: SurrogateNet, param: SmoothD
          the next one follows (at most `max_bursts` kept per cycle); one that
          did not is rolled back (design and Adam state) and retried with half
          the step, at most `max_tries` rejections per cycle;
-      3. fallback: when the surrogate's power-transmission error on the last
-         verified design (power_error, mean over the designs) exceeds
-         `max_error`, the next cycle takes `fallback_steps` plain FDTD steps
-         before its bursts.
+      3. fallback: the FDTD step of 1. also gives the true spectrum at its
+         design, so the surrogate's power-transmission error there
+         (power_error, mean over the designs) is known at the cost of one
+         prediction; above `max_error` the cycle makes no burst and the next
+         one takes `fallback_steps` plain FDTD steps, so while the network
+         is off the loop is the plain adjoint loop.
     Every FDTD spectrum feeds `tuner` (online fine-tuning). Iterations are
     design updates: FDTD steps and kept surrogate steps count toward `iters`,
     rolled-back bursts do not. With `target`, records the wall-clock at which
@@ -865,11 +867,20 @@ def surrogate_loop(problem: FDTDDesignProblem, net: SurrogateNet, param: SmoothD
                 tuner.add(rho, T)
             _, g_sur = net.value_and_grad(rho, band_objective)
             delta = g - g_sur
+            perr_fdtd = float(np.mean(power_error(net.predict(rho), T)))
             opt.lr = lr
             z = opt.ascend(z, param.grad_z(z, g))
             it += 1
         if it >= iters:
             break
+        if perr_fdtd > max_error:  # 3. the surrogate sits this cycle out
+            n_plain = fallback_steps
+            log.append({"iter": it, "t": round(time.perf_counter() - t0, 3), "best": best_v,
+                        "objective": cur_v, "bursts_kept": 0, "bursts_rejected": 0,
+                        "power_error": perr_fdtd, "next_fdtd_steps": n_plain})
+            if tuner is not None:
+                tuner.tune()
+            continue
         # 2. corrected surrogate bursts, each verified
         step, kept, rejected, perr, vt = blr, 0, 0, 0.0, cur_v
         while kept < max_bursts and rejected < max_tries and it < iters:
@@ -897,7 +908,6 @@ def surrogate_loop(problem: FDTDDesignProblem, net: SurrogateNet, param: SmoothD
                 step *= 0.5
                 rejected += 1
                 n_reject += 1
-        # 3. fallback when the surrogate is off by more than max_error
         n_plain = fallback_steps if perr > max_error else 1
         log.append({"iter": it, "t": round(time.perf_counter() - t0, 3), "best": best_v,
                     "objective": cur_v, "bursts_kept": kept, "bursts_rejected": rejected,

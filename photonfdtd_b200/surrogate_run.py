@@ -57,7 +57,7 @@ def main(argv=None):
     p.add_argument("--traj-heldout", type=int, default=0,
                    help="of the trajectory designs, this many (the last whole batches) are "
                         "held out for evaluation")
-    p.add_argument("--loop-variants", default="3:1:1",
+    p.add_argument("--loop-variants", default="1:1:1",
                    help="surrogate loops to run, comma-separated FALLBACK:BURST_LR_MULT:MAX_BURSTS")
     p.add_argument("--data", default=None,
                    help="npz of cached spectra (T_train, T_heldout); written if absent")
