@@ -144,6 +144,39 @@ def default_checkpoint(n_steps: int, state_reals: int, design_cells: int) -> int
     return int(max(1, min(n_steps, round(k))))
 
 
+def checkpoint_bytes(n_steps: int, k: int, state_reals: int, design_cells: int,
+                     real_bytes: int) -> int:
+    """Stored bytes of the adjoint at spacing K: ceil(N/K) - 1 states plus a
+    ring of K steps x 2 reals per design cell."""
+    return (((n_steps + k - 1) // k - 1) * state_reals + k * 2 * design_cells) * real_bytes
+
+
+def choose_checkpoint(n_steps: int, state_reals: int, design_cells: int, real_bytes: int,
+                      budget_bytes: float) -> int:
+    """The largest K whose stored bytes fit `budget_bytes`: the fewest
+    segments, hence the least forward replay (K >= N: none at all). When no
+    K fits, the memory-minimising default_checkpoint."""
+    k0 = default_checkpoint(n_steps, state_reals, design_cells)
+    for segs in range(1, n_steps + 1):  # K = ceil(N / segs), largest first
+        k = (n_steps + segs - 1) // segs
+        if k < k0:
+            break
+        if checkpoint_bytes(n_steps, k, state_reals, design_cells, real_bytes) <= budget_bytes:
+            return k
+    return k0
+
+
+def default_memory_budget() -> float:
+    """Half of the device memory free now (0 without a CUDA device)."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return 0.5 * float(torch.cuda.mem_get_info()[0])
+    except Exception:  # noqa: BLE001 - no usable CUDA runtime: no budget
+        pass
+    return 0.0
+
+
 # --------------------------------------------------------------------------- #
 # The batch
 # --------------------------------------------------------------------------- #
@@ -151,13 +184,18 @@ class BatchTE:
     """One GPU batch of 2D TE instances with forward and adjoint passes.
 
     ``windows[k] = (i0, j0, n)`` is instance k's design window. ``checkpoint_every``
-    (K) trades memory for nothing else: the adjoint always replays the forward
+    (K) trades memory for replay time only: the adjoint replays the forward
     once between checkpoints; K >= n_steps stores no state at all and skips
-    the replay. The default K minimises stored bytes.
+    the replay. Results do not depend on K. The default is the largest K
+    whose stored bytes fit ``memory_budget`` (default: half of the device
+    memory free at construction): on a B200 a config-4 batch keeps its whole
+    33.5 GB ring and replays nothing; a batch that does not fit gets the
+    memory-minimising K.
     """
 
     def __init__(self, sims: Sequence, windows: Sequence[Tuple[int, int, int]],
-                 checkpoint_every: Optional[int] = None, tile_rows: int = 32):
+                 checkpoint_every: Optional[int] = None, tile_rows: int = 32,
+                 memory_budget: Optional[float] = None):
         if len(sims) == 0 or len(sims) != len(windows):
             raise ValueError("need one design window per simulation")
         wave_cache: Dict = {}
@@ -184,7 +222,9 @@ class BatchTE:
         self.ncell = int(sum(t["nx"] * t["ny"] for t in tabs))
         state = 3 * self.ncell + sum(psi_cells(t) for t in tabs)
         if checkpoint_every is None:
-            checkpoint_every = default_checkpoint(self.n_steps, state, self.n_design)
+            budget = default_memory_budget() if memory_budget is None else memory_budget
+            checkpoint_every = choose_checkpoint(self.n_steps, state, self.n_design,
+                                                 np.dtype(self.npdt).itemsize, budget)
         self._L = N.lib()
         L = self._L
         h = C.c_void_p()

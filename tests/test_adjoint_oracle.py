@@ -9,7 +9,8 @@ import pytest
 
 import photonfdtd_b200 as pf
 from photonfdtd_b200 import workloads as W
-from photonfdtd_b200.batch import default_checkpoint, line_dft, value_and_grad_eps
+from photonfdtd_b200.batch import (checkpoint_bytes, choose_checkpoint, default_checkpoint,
+                                   line_dft, value_and_grad_eps)
 from oracle.adjoint2d import TEAdjointRun, objective, objective_cotangent
 from oracle.fdtd_oracle import EPS0, OracleRun
 
@@ -150,3 +151,20 @@ def test_default_checkpoint_balances_states_and_ring():
     assert 300 < k < 700
     assert default_checkpoint(10, 10, 1_000_000) == 1
     assert default_checkpoint(10, 10 ** 9, 1) == 10
+
+
+def test_checkpoint_spacing_spends_the_memory_budget():
+    N, state, D, rb = 4000, 110_000_000, 256 * 64 * 64, 4
+    ring_all = N * 2 * D * rb                      # 33.5 GB: no checkpoints at all
+    assert checkpoint_bytes(N, N, state, D, rb) == ring_all
+    assert choose_checkpoint(N, state, D, rb, 90e9) == N
+    k0 = default_checkpoint(N, state, D)
+    assert choose_checkpoint(N, state, D, rb, 0.0) == k0   # nothing fits: minimal memory
+    for budget in (8e9, 12e9, 20e9, 30e9):
+        k = choose_checkpoint(N, state, D, rb, budget)
+        assert k0 <= k < N
+        assert checkpoint_bytes(N, k, state, D, rb) <= budget
+        # the next larger spacing (one segment fewer) would not fit
+        segs = (N + k - 1) // k
+        k_up = (N + segs - 2) // (segs - 1)
+        assert checkpoint_bytes(N, k_up, state, D, rb) > budget
