@@ -264,6 +264,19 @@ int pfb_set_dft(pf_batch *b, int n_freq, const double *phase);
  * updates tile_rows / 8 consecutive rows). */
 int pfb_finalize(pf_batch *b, int checkpoint_every, int tile_rows);
 
+/* Re-lays the work list at another tile height (8, 16 or 32 x rows) after
+ * pfb_finalize; allocates nothing (the tile buffer is sized for 8). Results
+ * do not depend on the tile height. No counterpart in the reference (its
+ * GPU path launches one thread per cell, rust/src/cuda.rs:298-341). */
+int pfb_set_tile_rows(pf_batch *b, int tile_rows);
+/* The tile-height autotuner: for 8, 16 and 32 rows, runs trial_steps forward
+ * steps (clamped to the checkpoint spacing and n_steps) once to capture
+ * their graph and once timed by CUDA events on the batch stream; writes the
+ * three ms per step to ms_per_step[3], keeps the fastest height (*best_rows)
+ * and resets the state (fields, ring, DFT sums): call it before pfb_forward.
+ * No counterpart in the reference. */
+int pfb_tune_tiles(pf_batch *b, int trial_steps, float *ms_per_step, int *best_rows);
+
 /* Replaces the design-window coefficients of every instance from a packed
  * host array (n_design reals). */
 int pfb_set_design_ce(pf_batch *b, const void *ce_design);

@@ -77,6 +77,8 @@ SIGNATURES = {
                                   C.c_int, _pdbl]),
     "pfb_set_dft": (C.c_int, [_vp, C.c_int, _pdbl]),
     "pfb_finalize": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "pfb_set_tile_rows": (C.c_int, [_vp, C.c_int]),
+    "pfb_tune_tiles": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "pfb_set_design_ce": (C.c_int, [_vp, _vp]),
     "pfb_forward": (C.c_int, [_vp]),
     "pfb_adjoint": (C.c_int, [_vp, _pdbl]),

@@ -190,12 +190,16 @@ class BatchTE:
     whose stored bytes fit ``memory_budget`` (default: half of the device
     memory free at construction): on a B200 a config-4 batch keeps its whole
     33.5 GB ring and replays nothing; a batch that does not fit gets the
-    memory-minimising K.
+    memory-minimising K. ``tile_rows`` is the x height of a work tile (8, 16
+    or 32 rows by 32 cells); "auto" (the default) lets the autotuner time a
+    short forward chunk at each height on this batch and keep the fastest
+    (``tile_ms_per_step`` records the three timings). Results do not depend
+    on the tile height.
     """
 
     def __init__(self, sims: Sequence, windows: Sequence[Tuple[int, int, int]],
-                 checkpoint_every: Optional[int] = None, tile_rows: int = 32,
-                 memory_budget: Optional[float] = None):
+                 checkpoint_every: Optional[int] = None, tile_rows="auto",
+                 memory_budget: Optional[float] = None, tune_steps: int = 64):
         if len(sims) == 0 or len(sims) != len(windows):
             raise ValueError("need one design window per simulation")
         wave_cache: Dict = {}
@@ -233,7 +237,17 @@ class BatchTE:
                              self.n_steps, C.byref(h)), None, batch=True)
         self.h = h
         try:
-            self._setup(tabs, wave_cache, phase_cache, int(checkpoint_every), int(tile_rows))
+            auto = tile_rows == "auto"
+            self._setup(tabs, wave_cache, phase_cache, int(checkpoint_every),
+                        32 if auto else int(tile_rows))
+            self.tile_ms_per_step = None
+            self.tile_rows = 32 if auto else int(tile_rows)
+            if auto:
+                ms = (C.c_float * 3)()
+                best = C.c_int(0)
+                self._chk(L.pfb_tune_tiles(h, int(tune_steps), ms, C.byref(best)))
+                self.tile_rows = int(best.value)
+                self.tile_ms_per_step = {r: float(m) for r, m in zip((8, 16, 32), ms)}
         except Exception:
             self.close()
             raise

@@ -74,6 +74,8 @@ struct pf_batch {
   Inst* d_inst = nullptr;
   TileRec* d_tiles = nullptr;
   int ntiles = 0;
+  int tile_rows = 32;
+  size_t tile_cap = 0;  // TileRec slots of d_tiles (the 8-row list, the longest)
   void *Ex = nullptr, *Ey = nullptr, *Hz = nullptr, *ce = nullptr;
   void* coef[8] = {};
   void* psi[4] = {};
@@ -517,6 +519,119 @@ int pfb_set_dft(pf_batch* b, int n_freq, const double* phase) {
   return PF_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The work list at a tile height of tile_rows rows (x) by 32 cells (y),
+// every instance's tiles in order.
+std::vector<TileRec> make_tiles(const pf_batch* b, int tile_rows) {
+  std::vector<TileRec> tiles;
+  for (int k = 0; k < b->n_inst; ++k) {
+    const Inst& I = b->inst[k];
+    for (int i0 = 0; i0 < I.nx; i0 += tile_rows)
+      for (int j0 = 0; j0 < I.ny; j0 += 32) {
+        TileRec tr;
+        tr.base = I.off + (long long)i0 * I.pitch + j0;
+        tr.nx = I.nx;
+        tr.ny = I.ny;
+        tr.pitch = I.pitch;
+        tr.i0 = i0;
+        tr.j0 = j0;
+        tr.ox = I.ox + i0;
+        tr.oy = I.oy + j0;
+        tr.k = k;
+        tr.wdi = I.di0 - i0;
+        tr.wdj = I.dj0 - j0;
+        tr.wdn = I.dn;
+        tr.pad[0] = 0;
+        tiles.push_back(tr);
+      }
+  }
+  return tiles;
+}
+
+int set_tile_rows(pf_batch* b, int tile_rows) {
+  const std::vector<TileRec> tiles = make_tiles(b, tile_rows);
+  if (tiles.size() > b->tile_cap) return bfail(b, PF_ERR_INVALID, "tile list exceeds its buffer");
+  B_CUDA(b, cudaMemcpyAsync(b->d_tiles, tiles.data(), tiles.size() * sizeof(TileRec),
+                            cudaMemcpyHostToDevice, b->stream));
+  B_CUDA(b, cudaStreamSynchronize(b->stream));  // before `tiles` goes
+  destroy_graphs(b);  // captured with the old grid and row count
+  b->ntiles = (int)tiles.size();
+  b->rows = tile_rows / kWarps;
+  b->tile_rows = tile_rows;
+  return PF_OK;
+}
+
+template <typename T>
+int tune_tiles_t(pf_batch* b, int trial, float* ms3, int* best) {
+  static const int cand[3] = {8, 16, 32};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  int rc = PF_OK;
+  if (cudaEventCreate(&ev[0]) != cudaSuccess || cudaEventCreate(&ev[1]) != cudaSuccess)
+    rc = bfail(b, PF_ERR_CUDA, "cudaEventCreate failed");
+  int bi = 2;
+  for (int c = 0; c < 3 && !rc; ++c) {
+    if ((rc = set_tile_rows(b, cand[c]))) break;
+    for (int rep = 0; rep < 2 && !rc; ++rep) {  // rep 0 captures the chunk's graph
+      if ((rc = zero_state(b)) || (rc = set_base(b, 0))) break;
+      if (rep && cudaEventRecord(ev[0], b->stream) != cudaSuccess) {
+        rc = bfail(b, PF_ERR_CUDA, "cudaEventRecord failed");
+        break;
+      }
+      if ((rc = run_chunk<T>(b, 0, trial))) break;
+      if (rep && cudaEventRecord(ev[1], b->stream) != cudaSuccess) {
+        rc = bfail(b, PF_ERR_CUDA, "cudaEventRecord failed");
+        break;
+      }
+    }
+    if (rc) break;
+    float ms = 0.f;
+    if (cudaEventSynchronize(ev[1]) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, ev[0], ev[1]) != cudaSuccess) {
+      rc = bfail(b, PF_ERR_CUDA, "tile timing failed");
+      break;
+    }
+    ms3[c] = ms / trial;
+    if (ms3[c] < ms3[bi] || c == 0) bi = c;
+  }
+  for (cudaEvent_t e : ev)
+    if (e) cudaEventDestroy(e);
+  if (rc) return rc;
+  if ((rc = set_tile_rows(b, cand[bi]))) return rc;
+  // the trial runs left fields, ring and DFT lines behind: start clean
+  if ((rc = zero_state(b))) return rc;
+  B_CUDA(b, cudaMemsetAsync(b->acc, 0, (size_t)b->nline * b->n_freq * 16, b->stream));
+  B_CUDA(b, cudaStreamSynchronize(b->stream));
+  b->fwd_done = false;
+  b->ring_last = false;
+  *best = cand[bi];
+  return PF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pfb_set_tile_rows(pf_batch* b, int tile_rows) {
+  if (!b) return PF_ERR_INVALID;
+  if (!b->finalized) return bfail(b, PF_ERR_STATE, "pfb_set_tile_rows before pfb_finalize");
+  if (tile_rows != 8 && tile_rows != 16 && tile_rows != 32)
+    return bfail(b, PF_ERR_INVALID, "tile_rows must be 8, 16 or 32");
+  return set_tile_rows(b, tile_rows);
+}
+
+int pfb_tune_tiles(pf_batch* b, int trial_steps, float* ms_per_step, int* best_rows) {
+  if (!b) return PF_ERR_INVALID;
+  if (!b->finalized) return bfail(b, PF_ERR_STATE, "pfb_tune_tiles before pfb_finalize");
+  if (trial_steps < 1 || !ms_per_step || !best_rows)
+    return bfail(b, PF_ERR_INVALID, "pfb_tune_tiles: bad arguments");
+  const int trial = (int)std::min<long long>(trial_steps, std::min<long long>(b->ckpt, b->n_steps));
+  return b->rb == 4 ? tune_tiles_t<float>(b, trial, ms_per_step, best_rows)
+                    : tune_tiles_t<double>(b, trial, ms_per_step, best_rows);
+}
+
 int pfb_finalize(pf_batch* b, int checkpoint_every, int tile_rows) {
   if (!b) return PF_ERR_INVALID;
   if (b->finalized) return bfail(b, PF_ERR_STATE, "pfb_finalize called twice");
@@ -573,24 +688,6 @@ int pfb_finalize(pf_batch* b, int checkpoint_every, int tile_rows) {
     for (int q = 0; q < 8; ++q)
       coefp[q].insert(coefp[q].end(), b->h_coef[q][k].begin(), b->h_coef[q][k].end());
     for (int j = 0; j < I.ny; ++j) lcell.push_back(I.off + (long long)I.line_i * I.pitch + j);
-    for (int i0 = 0; i0 < I.nx; i0 += tile_rows)
-      for (int j0 = 0; j0 < I.ny; j0 += 32) {
-        TileRec tr;
-        tr.base = I.off + (long long)i0 * I.pitch + j0;
-        tr.nx = I.nx;
-        tr.ny = I.ny;
-        tr.pitch = I.pitch;
-        tr.i0 = i0;
-        tr.j0 = j0;
-        tr.ox = I.ox + i0;
-        tr.oy = I.oy + j0;
-        tr.k = k;
-        tr.wdi = I.di0 - i0;
-        tr.wdj = I.dj0 - j0;
-        tr.wdn = I.dn;
-        tr.pad[0] = 0;
-        tiles.push_back(tr);
-      }
     b->ncell += (long long)I.nx * I.pitch;
     b->ncell_real += (long long)I.nx * I.ny;
     b->nx_tot += I.nx;
@@ -599,11 +696,16 @@ int pfb_finalize(pf_batch* b, int checkpoint_every, int tile_rows) {
     b->nline += I.ny;
     std::vector<char>().swap(b->h_ce[k]);
   }
-  if ((long long)tiles.size() >= (1LL << 31)) return bfail(b, PF_ERR_INVALID, "too many tiles");
+  tiles = make_tiles(b, tile_rows);
+  b->tile_cap = make_tiles(b, 8).size();
+  if ((long long)b->tile_cap >= (1LL << 31)) return bfail(b, PF_ERR_INVALID, "too many tiles");
   b->ntiles = (int)tiles.size();
+  b->tile_rows = tile_rows;
   int rc;
   if ((rc = bup(b, (void**)&b->d_inst, b->inst.data(), b->inst.size() * sizeof(Inst)))) return rc;
-  if ((rc = bup(b, (void**)&b->d_tiles, tiles.data(), tiles.size() * sizeof(TileRec)))) return rc;
+  if ((rc = balloc(b, (void**)&b->d_tiles, b->tile_cap * sizeof(TileRec)))) return rc;
+  B_CUDA(b, cudaMemcpyAsync(b->d_tiles, tiles.data(), tiles.size() * sizeof(TileRec),
+                            cudaMemcpyHostToDevice, b->stream));
   if ((rc = bup(b, &b->ce, cep.data(), cep.size()))) return rc;
   for (int q = 0; q < 8; ++q)
     if ((rc = bup(b, &b->coef[q], coefp[q].data(), coefp[q].size()))) return rc;

@@ -91,6 +91,35 @@ def test_checkpoint_spacing_changes_nothing():
     assert outs[0][2]["segments"] == 200 and outs[-1][2]["segments"] == 1
 
 
+def test_tile_autotuner_changes_nothing():
+    """The default tile height comes from timing 8, 16 and 32 rows on the
+    batch itself; whichever it keeps, and after an explicit retile, the DFT
+    and the gradient equal a fixed-height batch's bit for bit."""
+    sims, _, wins = _sims("float32", 150)
+    fixed = BatchTE(sims, wins, tile_rows=32)
+    auto = BatchTE(sims, wins)
+    L = N.lib()
+    try:
+        assert auto.tile_rows in (8, 16, 32)
+        assert set(auto.tile_ms_per_step) == {8, 16, 32}
+        assert all(m > 0 for m in auto.tile_ms_per_step.values())
+        assert auto.tile_ms_per_step[auto.tile_rows] == min(auto.tile_ms_per_step.values())
+        F0 = fixed.forward()
+        g0 = fixed.adjoint(objective_cotangent(F0))
+        F1 = auto.forward()
+        assert np.array_equal(F1, F0)
+        assert np.array_equal(auto.adjoint(objective_cotangent(F1)), g0)
+        for rows in (8, 16):
+            assert L.pfb_set_tile_rows(auto.h, rows) == N.PF_OK
+            F2 = auto.forward()
+            assert np.array_equal(F2, F0)
+            assert np.array_equal(auto.adjoint(objective_cotangent(F2)), g0)
+        assert L.pfb_set_tile_rows(auto.h, 12) == N.PF_ERR_INVALID
+    finally:
+        fixed.close()
+        auto.close()
+
+
 def test_gradient_matches_central_differences():
     """dJ/drho against (J(rho + h) - J(rho - h)) / 2h, h = 1e-4, float64, on 32
     pixels (default_rng(5)); each forward perturbs one pixel per instance."""
