@@ -209,6 +209,24 @@ int pf_flux_plane_noalloc(int real_bytes, int nx, int ny, int nz,
                           double dA, double dt, double *out, void *stream);
 const char *pf_noalloc_last_error(void);
 
+/* ----------------------------------------------------------------------
+ * Subpixel permittivity on the GPU (replaces the host precompute of
+ * src/photonfdtd/smoothing.py:87-172 for scenes made of boxes).
+ * Grid nx x ny x nz, `factor` sub-cells per resolved axis; the scene is the
+ * background permittivity overwritten, in order, by n_box boxes, box s
+ * covering the fine sub-cells [spans[6s], spans[6s+1]) x [spans[6s+2],
+ * spans[6s+3]) x [spans[6s+4], spans[6s+5]) with eps_box[s] (fine index i
+ * is native cell i / factor on a resolved axis; a collapsed axis has one
+ * fine cell). hx, hy, hz: the gradient spacing (the cell size) of each
+ * resolved axis. Writes eps_xx, eps_yy, eps_zz (nx*ny*nz each, C order, 4- or
+ * 8-byte reals per out_bytes) to host memory, bit for bit the reference's
+ * numpy result. Allocates and frees its own device scratch; synchronous.
+ * Error text: pf_smooth_last_error(). */
+int pf_smooth_boxes(int nx, int ny, int nz, int factor, double background, int n_box,
+                    const int32_t *spans, const double *eps_box, double hx, double hy,
+                    double hz, int out_bytes, void *out_xx, void *out_yy, void *out_zz);
+const char *pf_smooth_last_error(void);
+
 /* ------------------------------------------------------------------------
  * Batched 2D TE engine with a discrete adjoint (pf_batch).
  *

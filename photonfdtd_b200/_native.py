@@ -77,6 +77,9 @@ SIGNATURES = {
                                   C.c_int, _pdbl]),
     "pfb_set_dft": (C.c_int, [_vp, C.c_int, _pdbl]),
     "pfb_finalize": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "pf_smooth_boxes": (C.c_int, [C.c_int] * 4 + [C.c_double, C.c_int, _vp, _vp] +
+                        [C.c_double] * 3 + [C.c_int, _vp, _vp, _vp]),
+    "pf_smooth_last_error": (C.c_char_p, []),
     "pfb_set_tile_rows": (C.c_int, [_vp, C.c_int]),
     "pfb_tune_tiles": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int)]),
     "pfb_set_design_ce": (C.c_int, [_vp, _vp]),

@@ -166,6 +166,12 @@ class Simulation:
         if self._eps_r_custom:
             eps = self.eps_r
             return (eps, eps, eps)
+        from .smoothing import device_available, smooth_permittivity_device
+        if device_available() and all(hasattr(st, "index_slices") for st in self.structures):
+            # on the GPU, bit for bit the host result (boxes only)
+            return smooth_permittivity_device(self.grid, self.structures, background_eps=1.0,
+                                              factor=self.subpixel_factor,
+                                              dtype=self.dtypes["eps_r"])
         return smooth_permittivity(self.grid, self.structures, background_eps=1.0,
                                    factor=self.subpixel_factor, dtype=self.dtypes["eps_r"])
 

@@ -7,6 +7,10 @@ normalised gradient of eps_a; eps_ii = eps_a + (eps_h - eps_a) * n_i^2. The
 means use numpy's block mean over the reshaped sub-cell axes, so the values
 are bit-identical to the reference's. Box structures rasterise through index
 ranges instead of full boolean masks.
+
+smooth_permittivity_device computes the same tensor on the GPU
+(pf_smooth_boxes) for scenes made of boxes, bit for bit equal to
+smooth_permittivity; Simulation uses it whenever a CUDA device is present.
 """
 from __future__ import annotations
 
@@ -72,3 +76,54 @@ def smooth_permittivity(grid, structures, background_eps: float = 1.0, factor: i
     normal = [g * inv for g in grads]
     delta = eps_h - eps_a
     return tuple((eps_a + delta * normal[a] ** 2).astype(dtype, copy=False) for a in range(3))
+
+
+def box_spans(grid, structures, factor: int):
+    """(spans int32 (m, 6), eps float64 (m,)) of the boxes on the fine grid
+    (half-open index ranges per axis), in stamping order; None when a
+    structure is not a box (no index_slices)."""
+    if not all(hasattr(s, "index_slices") for s in structures):
+        return None
+    xf, yf, zf = _fine_coords(grid, factor)
+    duck = SimpleNamespace(shape=(xf.size, yf.size, zf.size), coords=(xf, yf, zf))
+    spans, eps = [], []
+    for s in structures:
+        sl = s.index_slices(duck)
+        if sl is None:
+            continue
+        spans.append([v for x in sl for v in (x.start, x.stop)])
+        eps.append(float(s.medium.eps_r))
+    return np.array(spans, np.int32).reshape(-1, 6), np.array(eps, np.float64)
+
+
+def device_available() -> bool:
+    try:
+        import torch
+        return bool(torch.cuda.is_available())
+    except Exception:  # noqa: BLE001 - no CUDA runtime
+        return False
+
+
+def smooth_permittivity_device(grid, structures, background_eps: float = 1.0, factor: int = 3,
+                               dtype=np.float64) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """smooth_permittivity for scenes made of boxes, on the GPU."""
+    from . import _native as N
+    if factor < 1:
+        raise ValueError("factor must be >= 1")
+    bs = box_spans(grid, structures, factor)
+    if bs is None:
+        raise NotImplementedError("GPU smoothing takes box structures only")
+    spans, eps = bs
+    dt = np.dtype(dtype)
+    if dt not in (np.dtype(np.float32), np.dtype(np.float64)):
+        raise ValueError("dtype must be float32 or float64")
+    out = tuple(np.empty(grid.shape, dt) for _ in range(3))
+    h = [grid.cell_size[a] if grid.shape[a] > 1 else 1.0 for a in range(3)]
+    L = N.lib()
+    rc = L.pf_smooth_boxes(*grid.shape, int(factor), float(background_eps), int(len(eps)),
+                           spans.ctypes.data if len(eps) else None,
+                           eps.ctypes.data if len(eps) else None, *[float(v) for v in h],
+                           dt.itemsize, *[o.ctypes.data for o in out])
+    if rc != N.PF_OK:
+        raise N.NativeError(rc, L.pf_smooth_last_error().decode())
+    return out
