@@ -85,13 +85,21 @@ def box_spans(grid, structures, factor: int):
     if not all(hasattr(s, "index_slices") for s in structures):
         return None
     xf, yf, zf = _fine_coords(grid, factor)
-    duck = SimpleNamespace(shape=(xf.size, yf.size, zf.size), coords=(xf, yf, zf))
+    nx = grid.shape[0]
+    # slab_means stamps one x-slab of factor fine cells at a time; a slab one
+    # cell thick (factor 1) takes the box rasterisation's collapsed-axis rule
+    # (covered in full when the box's x extent straddles 0, else not at all),
+    # so its x span is all or nothing, as on the host
+    thin = nx > 1 and factor == 1
+    xd = xf[:1] if thin else xf
+    duck = SimpleNamespace(shape=(xd.size, yf.size, zf.size), coords=(xd, yf, zf))
     spans, eps = [], []
     for s in structures:
         sl = s.index_slices(duck)
         if sl is None:
             continue
-        spans.append([v for x in sl for v in (x.start, x.stop)])
+        xs = (0, nx) if thin else (sl[0].start, sl[0].stop)
+        spans.append([*xs, sl[1].start, sl[1].stop, sl[2].start, sl[2].stop])
         eps.append(float(s.medium.eps_r))
     return np.array(spans, np.int32).reshape(-1, 6), np.array(eps, np.float64)
 

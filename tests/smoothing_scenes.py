@@ -28,4 +28,6 @@ def scenes():
                                      precision="float64", subpixel_factor=2)),
         ("2d_xy", scene_2d((2.0e-6, 1.5e-6, 0.0))),
         ("2d_xz", scene_2d((2.0e-6, 0.0, 1.5e-6))),
+        ("3d_factor1", W.config2(pf, interior=24, n_boxes=12, n_steps=5, subpixel_factor=1)),
+        ("3d_factor4", W.config2(pf, interior=24, n_boxes=12, n_steps=5, subpixel_factor=4)),
     ]
