@@ -572,14 +572,29 @@ int sample_monitors(pf_engine* e, long long s, int lvl) {
         m.r, (T*)m.ring, m.pending, f, e->ny, e->nz);
     m.pending++;
   }
-  for (FluxMon& fl : e->fluxes) {
-    if (fl.pending == fl.ring_cap) {
-      int rc = flush_monitors<T>(e);
-      if (rc) return rc;
+  // every flux plane samples every step: up to kFluxBatch planes per launch
+  for (size_t q0 = 0; q0 < e->fluxes.size(); q0 += kFluxBatch) {
+    const size_t q1 = std::min(e->fluxes.size(), q0 + (size_t)kFluxBatch);
+    for (size_t q = q0; q < q1; ++q)
+      if (e->fluxes[q].pending == e->fluxes[q].ring_cap) {
+        int rc = flush_monitors<T>(e);
+        if (rc) return rc;
+        break;
+      }
+    FluxBatch fb;
+    memset(&fb, 0, sizeof fb);
+    int maxblk = 1;
+    for (size_t q = q0; q < q1; ++q) {
+      FluxMon& fl = e->fluxes[q];
+      fb.p[q - q0] = fl.p;
+      fb.partial[q - q0] = fl.partial;
+      fb.slot[q - q0] = fl.pending;
+      maxblk = std::max(maxblk, fl.p.nblk);
     }
     LaunchScope ls(e, 2);
-    k_flux_sample<T><<<fl.p.nblk, 256, 0, e->stream>>>(fl.p, fl.partial, fl.pending, f, e->ny, e->nz);
-    fl.pending++;
+    k_flux_sample_batch<T><<<dim3(maxblk, (unsigned)(q1 - q0)), 256, 0, e->stream>>>(fb, f, e->ny,
+                                                                                     e->nz);
+    for (size_t q = q0; q < q1; ++q) e->fluxes[q].pending++;
   }
   return PF_OK;
 }

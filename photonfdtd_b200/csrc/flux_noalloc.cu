@@ -1,7 +1,7 @@
 // flux_noalloc.cu - plane Poynting flux with no device allocation.
 //
 // pf_flux_plane_noalloc is the flux monitor's per-step reduction
-// (k_flux_sample + the fixed-order fold of k_flux_flush) as a standalone
+// (k_flux_sample_batch + the fixed-order fold of k_flux_flush) as a standalone
 // call for programs that must not allocate device memory on the call path.
 // Typical examples: a process whose device memory is owned by another
 // allocator (a framework's caching pool, or a serving process that reserved

@@ -141,10 +141,26 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return v;
 }
 
+// Flux planes sampled by one launch (up to kFluxBatch): blockIdx.y picks
+// the plane; block x of a plane sums S = E_t1 H_t2 - E_t2 H_t1 (rounded in
+// the field type, simulation.py:1440-1459) over the plane's cells
+// [256 x, 256 x + 256) in row-major (n0, n1) order with block_sum, and
+// stores the partial in the plane's ring slot; k_flux_flush folds the
+// partials in block order. Blocks past a plane's own count return before
+// any barrier, as a whole.
+constexpr int kFluxBatch = 8;
+struct FluxBatch {
+  FluxPlane p[kFluxBatch];
+  double* partial[kFluxBatch];
+  int slot[kFluxBatch];
+};
+
 template <typename T>
-__global__ void __launch_bounds__(256) k_flux_sample(FluxPlane p, double* partial, int slot,
-                                                     Fields6<T> fields, int ny, int nz) {
+__global__ void __launch_bounds__(256) k_flux_sample_batch(FluxBatch b, Fields6<T> fields, int ny,
+                                                           int nz) {
   __shared__ double sh[8];
+  const FluxPlane& p = b.p[blockIdx.y];
+  if ((int)blockIdx.x >= p.nblk) return;  // uniform over the block
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double v = 0.0;
   if (t < (long long)p.n0 * p.n1) {
@@ -166,7 +182,7 @@ __global__ void __launch_bounds__(256) k_flux_sample(FluxPlane p, double* partia
     v = (double)s;
   }
   v = block_sum<T>(v, sh);
-  if (threadIdx.x == 0) partial[(long long)slot * p.nblk + blockIdx.x] = v;
+  if (threadIdx.x == 0) b.partial[blockIdx.y][(long long)b.slot[blockIdx.y] * p.nblk + blockIdx.x] = v;
 }
 
 template <typename T>
