@@ -183,6 +183,23 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def max_over_ranks(x: float, dist=None, device: str = "cuda") -> float:
+    """The largest of every rank's x (every rank calls it, in the same order);
+    x itself without a process group."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world: int, cells: int, steps: int, ms: float) -> float:
+    """Whole-job Mcell-updates/s: world replicas of `cells` cells advanced
+    `steps` steps in `ms` milliseconds (the slowest rank's time)."""
+    return world * cells * steps / (ms / 1e3) / 1e6
+
+
 def bf16_peak():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -416,12 +433,10 @@ def main():
     pos += args.steps
     ms = ev0.elapsed_time(ev1)
     launches, _ = eng.read_profile(reset=True)
+    ms = max_over_ranks(ms, dist)
     if dist is not None:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
         dist.barrier()
-    value = world * alg["ncell"] * args.steps / (ms / 1e3) / 1e6
+    value = job_rate(world, alg["ncell"], args.steps, ms)
 
     # roofline of the step kernels: a second pass with per-launch events
     eng.set_profiling(True)
@@ -463,11 +478,9 @@ def main():
         wall = time.perf_counter() - t0
         h2d = e2_upload_bytes(t)
         e2.close()
-        if dist is not None:
-            tt = torch.tensor([wall], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            wall = float(tt.item())
-        e2e = {"value": round(world * alg["ncell"] * args.steps / wall / 1e6, 2), "unit": UNIT,
+        wall = max_over_ranks(wall, dist)
+        e2e = {"value": round(job_rate(world, alg["ncell"], args.steps, wall * 1e3), 2),
+               "unit": UNIT,
                "h2d_bytes_per_step": int(h2d / args.steps),
                "d2h_bytes_per_step": int(d2h / args.steps),
                "what": f"engine create + table upload from host memory, {args.steps} steps, "
@@ -488,9 +501,7 @@ def main():
         adj = adjoint_bench(max(1, args.adjoint_iters), rank == 0 and world == 1 and
                             not args.no_cpu_baseline)
         if dist is not None:
-            tt = torch.tensor([adj["value"]], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            adj["value"] = round(float(tt.item()), 3)
+            adj["value"] = round(max_over_ranks(adj["value"], dist), 3)
             adj["scaling"] = "weak (one batch per rank)"
         line["adjoint"] = adj
     if rank == 0 and world == 1 and not args.no_reference_gpu:
