@@ -5,7 +5,8 @@
 The reference keeps its Yee+CPML kernels as CUDA C source text inside
 rust/src/cuda.rs (the KERNEL_SRC raw string, compiled at run time by NVRTC
 with -DREAL=float|double). This recipe reads that text from the reference
-tree (default /root/reference), writes it to a temporary directory outside
+tree (located by baseline.locate: argument, PHOTONFDTD_REFERENCE, or a
+``reference`` directory beside the repository), writes it to a temporary directory outside
 the repository, and compiles it together with this project's host harness
 (launch.cu) into baseline/_ref/librefcuda_f32.so and librefcuda_f64.so,
 which are git-ignored. Nothing is built when the reference tree is absent.
@@ -31,7 +32,11 @@ def kernel_source(ref_root: str) -> str:
     return text[i:text.index(END, i)]
 
 
-def build(ref_root: str = "/root/reference", force: bool = False) -> list:
+def build(ref_root: str = None, force: bool = False) -> list:
+    from baseline.locate import reference_root
+    ref_root = reference_root(ref_root)
+    if ref_root is None:
+        return []
     src_file = os.path.join(ref_root, "rust", "src", "cuda.rs")
     if not os.path.exists(src_file):
         return []

@@ -24,9 +24,18 @@ measured through photonfdtd_b200.batch.value_and_grad_eps (host design in,
 host gradient out), with its forward / adjoint split and a CPU baseline of the
 NumPy forward + adjoint restatement on one instance.
 
---impl reference times the reference's CPU algorithm for the same workload:
-the NumPy restatement in oracle/ (the reference package itself is Python
-and not present where this runs), on a bounded sample of full-domain steps.
+--impl reference times the reference's own CPU implementation of the same
+workload: photonfdtd.Simulation(...).run() from the reference package
+installed in baseline/_ref (baseline/refcpu.py), its vectorised NumPy path on
+a bounded sample of full-domain steps, plus its Numba path (every core) on
+the non-dispersive variant it accepts. Where the package is absent it falls
+back to the NumPy restatement in oracle/ (kind "port").
+
+Other objects of the line: "e2e" (config 3 run end to end through the
+reference's own Simulation with backend="b200" from the plugin), "config2"
+(the 536^3 subpixel workload, with its own roofline), "error_vs_f64" (the
+float32 result against a float64 run of the same steps), "reference_gpu"
+(the reference's CUDA kernels compiled for this GPU) and "surrogate".
 """
 from __future__ import annotations
 
@@ -71,6 +80,14 @@ def parse():
                    help="time the config-4 gradient iteration alone (profiling)")
     p.add_argument("--adjoint-instances", type=int, default=256)
     p.add_argument("--adjoint-steps", type=int, default=4000)
+    p.add_argument("--no-numba", action="store_true",
+                   help="reference arm: skip the reference's Numba point")
+    p.add_argument("--no-config2", action="store_true",
+                   help="skip the 536^3 subpixel workload leg")
+    p.add_argument("--no-f64", action="store_true",
+                   help="skip the float64 error statement")
+    p.add_argument("--e2e-steps", type=int, default=3000,
+                   help="steps of the end-to-end Simulation.run() (config 3 runs 3000)")
     return p.parse_args()
 
 
@@ -285,6 +302,19 @@ def traffic_record(kernel_kind):
 
 # --------------------------------------------------------------------------- #
 def cpu_baseline(size, steps=2):
+    """The reference's own NumPy path (baseline/refcpu.py) on `steps` timed
+    full-domain steps of the workload, one core (NumPy ufuncs are
+    single-threaded); the oracle port where the reference is not installed."""
+    from baseline import locate
+    if locate.installed():
+        from baseline import refcpu
+        out = refcpu.numpy_config3(size, steps=steps)
+        out.pop("s_per_step", None)
+        return out
+    return cpu_baseline_port(size, steps)
+
+
+def cpu_baseline_port(size, steps=2):
     """The oracle (NumPy restatement of the reference CPU path) on full-domain
     steps of the same workload; one core (NumPy ufuncs are single-threaded)."""
     import photonfdtd_b200 as pf
@@ -302,7 +332,9 @@ def cpu_baseline(size, steps=2):
 
 
 def run_reference(args):
-    """--impl reference: rank 0 times the CPU algorithm; other ranks idle."""
+    """--impl reference: rank 0 times the reference's CPU implementation;
+    other ranks idle. Each timed step is one full-domain step of the
+    workload, bounded to 3 timed steps (about 9 s each on one core)."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
     k = max(1, min(args.steps, 3))
@@ -314,7 +346,168 @@ def run_reference(args):
             "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    from baseline import locate
+    if locate.installed() and not args.no_numba:
+        from baseline import refcpu
+        try:
+            line["numba"] = refcpu.numba_config3_plain(args.size, steps=k)
+        except Exception as exc:  # noqa: BLE001 - reported, not fatal
+            line["numba"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
     print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- #
+def e2e_bench(size: int, steps: int, world: int, dist) -> dict:
+    """Config 3 end to end through the call a user makes: the reference's
+    own photonfdtd.Simulation with backend="b200" (photonfdtd_b200.plugin),
+    scene on the host, Result back on the host; wall clock around run(),
+    which builds the tables, creates the engine (device memory, table upload),
+    steps, and reads the DFT and flux back. Falls back to this package's own
+    Simulation when the reference is not installed."""
+    import torch
+    import photonfdtd_b200 as pf
+    from photonfdtd_b200 import engine as E, plugin, workloads as W
+    from baseline.locate import import_reference
+    ref = import_reference()
+    if ref is not None:
+        plugin.install(ref)
+        sim = W.config3(ref, n_total=size, n_steps=steps, union_blocks=True, backend="b200")
+        api = "photonfdtd.Simulation(..., backend='b200').run() (reference package + plugin)"
+    else:
+        sim = W.config3(pf, n_total=size, n_steps=steps, union_blocks=True)
+        api = "photonfdtd_b200.Simulation(...).run()"
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = sim.run()
+    wall = time.perf_counter() - t0
+    st = dict(E.LAST_RUN)
+    if not (len(res.flux) == 6 and "d" in res.dft and np.isfinite(list(res.flux.values())).all()):
+        raise RuntimeError("e2e: Simulation.run() returned an incomplete Result")
+    wall = max_over_ranks(wall, dist)
+    return {"value": round(job_rate(world, size ** 3, steps, wall * 1e3), 2), "unit": UNIT,
+            "h2d_bytes_per_step": int(st["h2d_bytes"] / steps),
+            "d2h_bytes_per_step": int(st["d2h_bytes"] / steps),
+            "steps": steps, "wall_s": round(wall, 3),
+            "phases_s": {"tables": round(st["tables_s"], 3), "engine": round(st["create_s"], 3),
+                         "steps_and_readback": round(st["run_s"], 3)},
+            "what": f"{api}: config 3 at {size}^3 for {steps} steps, host scene in, "
+                    "Result (DFT + flux) out, wall clock"}
+
+
+def config2_bench(steps: int, warmup: int, world: int, dist) -> dict:
+    """Config 2: 536^3 cells, 64 boxes with subpixel smoothing (three per-cell
+    coefficient arrays), the Ex dipole and a 16-wavelength Ex/Ey/Hx/Hy DFT on
+    the z = 0 plane every step. The subpixel precompute runs on the GPU and is
+    timed separately."""
+    import torch
+    import photonfdtd_b200 as pf
+    from photonfdtd_b200 import workloads as W
+    from photonfdtd_b200.engine import B200Engine, build_tables
+    from photonfdtd_b200.smoothing import smooth_permittivity_device
+    sim = W.config2(pf, n_steps=warmup + 2 * steps + 8)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    smooth_permittivity_device(sim.grid, sim.structures, background_eps=1.0,
+                               factor=sim.subpixel_factor, dtype=np.float32)
+    smooth_s = time.perf_counter() - t0
+    t = build_tables(sim)
+    alg = algorithmic_bytes(t)
+    eng = B200Engine(t)
+    try:
+        st = torch.cuda.ExternalStream(eng.stream())
+        eng.advance(0, warmup)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        eng.advance(warmup, steps)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), dist)
+        eng.set_profiling(True)
+        eng.advance(warmup + steps, steps)
+        _, pms = eng.read_profile(reset=True)
+        eng.set_profiling(False)
+    finally:
+        eng.close()
+    step_ms = pms[0] / steps
+    peak, kind = peaks()
+    achieved = alg["per_cell"] * alg["ncell"] / (step_ms / 1e3) / 1e9
+    return {"workload": "config2: 536^3 cells (512^3 interior + 12-cell CPML) at 20 nm, "
+                        "float32, 64 seeded boxes eps U[1, 12.1], subpixel smoothing "
+                        "(factor 3, diagonal tensor: 3 coefficient arrays), Ex dipole, "
+                        "16-wavelength Ex/Ey/Hx/Hy DFT on the z = 0 plane every step",
+            "cells": alg["ncell"], "steps": steps,
+            "value": round(job_rate(world, alg["ncell"], steps, ms), 2), "unit": UNIT,
+            "ms_per_step": round(ms / steps, 4),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "peak_source": kind, "step_kernels_ms_per_step": round(step_ms, 4),
+                         "algorithmic_bytes_per_cell": round(alg["per_cell"], 2)},
+            "dft_ms_per_step": round((pms[2] + pms[3]) / steps, 4),
+            "smoothing_s": round(smooth_s, 3)}
+
+
+def f64_error_bench(sim, t, steps: int = 1000) -> dict:
+    """The float32 step's error against float64, two ways:
+    replica: the reduced config-3 scene (64^3, the full 3000 steps) against
+    the reference's own float64 NumPy run (tests/golden/ade3d_f64.npz);
+    full_size: the benchmark workload, `steps` steps in float32 against the
+    same steps of the engine's float64 path (within 1e-12 of NumPy float64 on
+    every golden scene)."""
+    import photonfdtd_b200 as pf
+    from photonfdtd_b200 import accuracy as A
+    from photonfdtd_b200 import workloads as W
+    from photonfdtd_b200.engine import B200Engine, build_tables
+    out = {}
+    gpath = os.path.join(ROOT, "tests", "golden", "ade3d_f64.npz")
+    if os.path.exists(gpath):
+        g = np.load(gpath)
+        rsim = W.config3(pf, n_total=64, block=8, n_steps=3000)
+        rsim.add_monitor(pf.FieldMonitor(name="mid", components=("Ex", "Ey", "Ez", "Hx", "Hy",
+                                                                 "Hz"), plane_z=0.0,
+                                         times=[1000 * rsim.dt, 2999 * rsim.dt]))
+        res = rsim.run()
+        worst = {"rel_max": 0.0, "rel_l2": 0.0}
+        for k in g.files:
+            if k.startswith("f/"):
+                _, mon, c = k.split("/")
+                a = np.asarray(res.fields[mon][c])
+            elif k.startswith("dft/"):
+                _, mon, c = k.split("/")
+                a = np.asarray(res.dft[mon][c])
+            else:
+                continue
+            e = A._pair(a, g[k])
+            worst = {q: max(worst[q], e[q]) for q in worst}
+        out["replica"] = {"scene": "config-3 recipe at 64^3, 3000 steps, float32, against the "
+                                   "reference's float64 NumPy run (tests/golden/ade3d_f64.npz)",
+                          **{q: float(f"{v:.3e}") for q, v in worst.items()}}
+    e32 = B200Engine(t)
+    e64 = B200Engine(build_tables(sim, np.float64))
+    try:
+        e32.advance(0, steps)
+        e64.advance(0, steps)
+        worst = {"rel_max": 0.0, "rel_l2": 0.0}
+        for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+            e = A._pair(e32.get(c), e64.get(c))
+            worst = {q: max(worst[q], e[q]) for q in worst}
+        for k, d in enumerate(t["dft"]):
+            for c in d["m"].components:
+                e = A._pair(e32.read_dft(k, c, d["omega"].size, d["counts"]),
+                            e64.read_dft(k, c, d["omega"].size, d["counts"]))
+                worst = {q: max(worst[q], e[q]) for q in worst}
+        fl = max(A._pair([e32.read_flux(k)], [e64.read_flux(k)])["rel_max"]
+                 for k in range(len(t["flux"])))
+    finally:
+        e32.close()
+        e64.close()
+    out["full_size"] = {"scene": f"the benchmark workload, {steps} steps, float32 against the "
+                                 "engine's float64 path (fields and DFT)",
+                        **{q: float(f"{v:.3e}") for q, v in worst.items()},
+                        "flux_rel": float(f"{fl:.3e}")}
+    return out
 
 
 # --------------------------------------------------------------------------- #
@@ -354,11 +547,29 @@ def adjoint_bench(iters: int, cpu: bool, n_inst: int = 256, n_steps: int = 4000)
     info = b.info()
     launches = (info["launches"] - l0) // (2 * iters)
     cells = b.ncell * b.n_steps
+    # algorithmic bytes per cell-step: Ex, Ey, Hz read + written and ce read
+    # (28 B in float32) plus each CPML psi entry read + written; the adjoint
+    # moves the same for its adjoint fields and psi, plus the stored
+    # design-window curls (2 reals per design cell per step)
+    from photonfdtd_b200.batch import psi_cells
+    s_b = np.dtype(b.npdt).itemsize
+    psi = sum(psi_cells(tb) for tb in b.tabs)
+    fwd_bytes = (7 * s_b * b.ncell + 2 * s_b * psi) * b.n_steps
+    adj_bytes = fwd_bytes + 2 * s_b * b.n_design * b.n_steps
+    peak, pkind = peaks()
     out = {"metric": "adjoint grad s/iter (256-instance batch)", "value": round(min(times), 3),
            "unit": "s/iter", "higher_is_better": False, "iters": iters,
            "workload": ADJ_WORKLOAD, "cells": b.ncell, "steps": b.n_steps,
            "forward_s": round(min(fwd), 3), "adjoint_s": round(min(adj), 3),
            "forward_gcell_per_s": round(cells / min(fwd) / 1e9, 2),
+           "roofline": {
+               "bound": "hbm", "unit": "GB/s", "peak": peak, "peak_source": pkind,
+               "forward": {"achieved": round(fwd_bytes / min(fwd) / 1e9, 1),
+                           "frac": round(fwd_bytes / min(fwd) / 1e9 / peak, 4),
+                           "bytes_per_cell_step": round(fwd_bytes / cells, 2)},
+               "adjoint": {"achieved": round(adj_bytes / min(adj) / 1e9, 1),
+                           "frac": round(adj_bytes / min(adj) / 1e9 / peak, 4),
+                           "bytes_per_cell_step": round(adj_bytes / cells, 2)}},
            "checkpoint_every": info["checkpoint_every"], "segments": info["segments"],
            "setup_s": round(setup, 2), "gpu_launches_per_iter": int(launches),
            "objective_sum": float(np.sum(vals)), "grad_max": float(np.max(np.abs(grad)))}
@@ -459,34 +670,16 @@ def main():
             "algorithmic_bytes_per_cell": round(alg["per_cell"], 2),
             "monitor_ms_per_step": round((pms[1] + pms[2] + pms[3]) / kp, 4)}
 
-    # end to end through the C ABI with host buffers: upload tables, step,
-    # read the monitor results back
+    eng.close()
+    err64 = None
+    if not args.no_f64:
+        err64 = f64_error_bench(sim, t)
+
+    # end to end through the public API with host data: the reference's own
+    # Simulation (backend="b200" through the plugin) for config 3's steps
     e2e = None
     if not args.no_e2e:
-        eng.close()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        e2 = B200Engine(t, kernel=kern)
-        e2.advance(0, args.steps)
-        d2h = 0
-        for k, d in enumerate(t["dft"]):
-            for c in d["m"].components:
-                d2h += e2.read_dft(k, c, d["omega"].size, d["counts"]).nbytes
-        for k in range(len(t["flux"])):
-            e2.read_flux(k)
-            d2h += 8
-        wall = time.perf_counter() - t0
-        h2d = e2_upload_bytes(t)
-        e2.close()
-        wall = max_over_ranks(wall, dist)
-        e2e = {"value": round(job_rate(world, alg["ncell"], args.steps, wall * 1e3), 2),
-               "unit": UNIT,
-               "h2d_bytes_per_step": int(h2d / args.steps),
-               "d2h_bytes_per_step": int(d2h / args.steps),
-               "what": f"engine create + table upload from host memory, {args.steps} steps, "
-                       "DFT + flux read-back, wall clock"}
-    else:
-        eng.close()
+        e2e = e2e_bench(args.size, args.e2e_steps, world, dist)
 
     line = {"metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -497,6 +690,10 @@ def main():
                        "l2": "state ~6 GB > 126 MB L2: inputs larger than L2, no flush"},
             "roofline": roof, "e2e": e2e, "gpu_launches": int(sum(launches)),
             "clocks": clk.summary()}
+    if err64 is not None:
+        line["error_vs_f64"] = err64
+    if not args.no_config2:
+        line["config2"] = config2_bench(min(args.steps, 20), 3, world, dist)
     if not args.no_adjoint:
         adj = adjoint_bench(max(1, args.adjoint_iters), rank == 0 and world == 1 and
                             not args.no_cpu_baseline)
@@ -516,25 +713,6 @@ def main():
     if rank == 0:
         print(json.dumps(line), flush=True)
 
-
-def e2e_upload_bytes(t) -> int:
-    n = 0
-    if t["ce_mode"] == 2:
-        n += t["word"].nbytes + t["table"].nbytes
-    else:
-        n += sum(a.nbytes for a in t["ce"])
-    for ax in t["cpml"]:
-        n += sum(a.nbytes for a in ax)
-    if t["ade"] is not None and t["ade"]["cell_word"] is not None:
-        n += t["ade"]["cell_word"].nbytes
-    s = t["sources"]
-    n += s["wave"].nbytes + s["amp"].nbytes + s["cell"].nbytes
-    for d in t["dft"]:
-        n += d["ph_e"].nbytes + d["ph_h"].nbytes
-    return n
-
-
-e2_upload_bytes = e2e_upload_bytes
 
 if __name__ == "__main__":
     main()

@@ -154,6 +154,28 @@ int pf_read_dft(pf_engine *eng, int mon, int comp, double *host_dst);
 /* Time-integrated flux of flux monitor mon (simulation.py:1403-1406). */
 int pf_read_flux(pf_engine *eng, int mon, double *host_dst);
 
+/* Overwrite one field component of the current time level from host memory
+ * (nx*ny*nz reals): the inverse of pf_read_field. The reference's engines
+ * expose no such call; with pf_read_field it lets a caller start from a
+ * state of its own (the reference's out-of-core stepper reloads fields the
+ * same way, src/photonfdtd/outofcore.py:12-22). */
+int pf_write_field(pf_engine *eng, int comp, const void *host_src);
+
+/* The whole stepping state as one blob, for checkpoints: the six current
+ * field components, the E and current H CPML psi arrays, and the
+ * polarisation levels P^n then P^(n-1) of dispersive cells, all in the real
+ * type. Monitor accumulators are not part of it. pf_state_bytes gives its
+ * size; pf_get_state copies it out (dst_on_device != 0: dst is a device
+ * pointer); pf_set_state copies it in and sets the step counter to `step`
+ * (the state is taken to be the one reached after `step` steps; pending
+ * monitor samples are folded first). This is the checkpoint pair of a
+ * time-reversed pass: the reference's gradient path keeps the same quantities
+ * between remat segments (src/photonfdtd/jaxbackend.py:511-570). */
+int pf_state_bytes(const pf_engine *eng, int64_t *bytes);
+int pf_get_state(pf_engine *eng, void *dst, int64_t bytes, int dst_on_device);
+int pf_set_state(pf_engine *eng, int64_t step, const void *src, int64_t bytes,
+                 int src_on_device);
+
 /* Steps advanced so far. */
 int pf_step(const pf_engine *eng, int64_t *step);
 
@@ -199,8 +221,12 @@ void pf_destroy(pf_engine *eng);
  * Scratch: the per-block partial sums live in one fixed device array of
  * 65,536 doubles (512 KB) per GPU that loads the library, kept until the
  * process exits; planes of more than 16,777,216 cells are rejected with
- * PF_ERR_INVALID. The first call on a device resolves that array's address
- * with the device current, so make the first call before any stream capture.
+ * PF_ERR_INVALID. Every call made outside a stream capture looks up that
+ * array's device address with the device current (a lookup, no allocation),
+ * so the address stays right after cudaDeviceReset reloads the module; a
+ * call inside a capture reuses the last address found on that device, so
+ * make the first call on a device before any stream capture (a first call
+ * inside one returns PF_ERR_STATE).
  * Every call shares the array and each call writes all partials it reads, so
  * no state carries between calls; calls that overlap on the GPU (other
  * streams or threads) race on it. Error text: pf_noalloc_last_error(). */

@@ -301,11 +301,13 @@ def _cls(o) -> str:
     return type(o).__name__
 
 
-def scene_tables(sim) -> dict:
+def scene_tables(sim, ce3=None) -> dict:
     """Everything the step loop consumes, rebuilt from the scene alone.
 
     Courant dt and step count (simulation.py:522-528), ce / per-component ce
-    (:953-969), ch (:954), CPML (:794-808), ADE media (:572-636).
+    (:953-969), ch (:954), CPML (:794-808), ADE media (:572-636). ``ce3``, if
+    given, replaces the subpixel per-component coefficients (a test that has
+    them already, pinned elsewhere, skips the host smoothing of a large grid).
     """
     grid = grid_of(sim.grid)
     dtype, mon_dtype = resolve_precision(sim.precision)
@@ -332,7 +334,9 @@ def scene_tables(sim) -> dict:
     # (simulation.py:953, :508-518 of the reference's eps_r setter)
     eps = np.asarray(sim.eps_r) if custom else stamp_eps(grid, structures, dtype)
     ce = (dt / (eps * EPS0)).astype(dtype, copy=False)
-    if custom:
+    if ce3 is not None:
+        ce3 = tuple(np.asarray(c, dtype=dtype) for c in ce3)
+    elif custom:
         ce3 = (ce, ce, ce)
     elif getattr(sim, "subpixel", False):
         comps = smooth_eps(grid, structures, int(sim.subpixel_factor), dtype)
@@ -415,8 +419,8 @@ class OracleRun:
     at (n+1)dt, then FieldMonitor / DFTMonitor / FluxMonitor in list order.
     """
 
-    def __init__(self, sim, n_steps: Optional[int] = None):
-        t = scene_tables(sim)
+    def __init__(self, sim, n_steps: Optional[int] = None, ce3=None):
+        t = scene_tables(sim, ce3=ce3)
         self.t = t
         g: OGrid = t["grid"]
         self.grid = g
@@ -634,6 +638,12 @@ class OracleRun:
                 self.flux[m.name] += self._flux(m) * self.dt
 
     # ---- driver ---- #
+    def set_fields(self, fields: Dict[str, np.ndarray]) -> None:
+        """Replace field components of the current state (the engine's
+        pf_write_field); CPML psi and polarisation state are left as they are."""
+        for c, arr in fields.items():
+            self.F[c][...] = np.asarray(arr, dtype=self.dtype)
+
     def advance(self, n: int) -> None:
         for _ in range(int(n)):
             s = self.step

@@ -59,6 +59,10 @@ SIGNATURES = {
     "pf_read_dft": (C.c_int, [_vp, C.c_int, C.c_int, _pdbl]),
     "pf_read_flux": (C.c_int, [_vp, C.c_int, _pdbl]),
     "pf_step": (C.c_int, [_vp, _pi64]),
+    "pf_write_field": (C.c_int, [_vp, C.c_int, _vp]),
+    "pf_state_bytes": (C.c_int, [_vp, _pi64]),
+    "pf_get_state": (C.c_int, [_vp, _vp, _i64, C.c_int]),
+    "pf_set_state": (C.c_int, [_vp, _i64, _vp, _i64, C.c_int]),
     "pf_check_finite": (C.c_int, [_vp]),
     "pf_device_bytes": (C.c_int, [_vp, _pi64]),
     "pf_stream": (C.c_int, [_vp, C.POINTER(_vp)]),

@@ -115,6 +115,7 @@ struct pf_engine {
   int hb0[3] = {}, hb1[3] = {}, eb0[3] = {}, eb1[3] = {};
   void* psiE[6] = {};
   void* psiH[2][6] = {};
+  long long npsiE[6] = {}, npsiH[6] = {};  // reals per psi array
   void* P = nullptr;
   long long plev = 0;  // reals per polarisation level
   void* media = nullptr;
@@ -364,6 +365,8 @@ int finalize_typed(pf_engine* e) {
                            (long long)e->nph[0] * ny * nz, (long long)e->nph[0] * ny * nz,
                            nx * e->nph[1] * nz};
   for (int q = 0; q < 6; ++q) {
+    e->npsiE[q] = eE[q];
+    e->npsiH[q] = eH[q];
     if ((rc = dalloc(e, &e->psiE[q], eE[q] * S))) return rc;
     for (int lvl = 0; lvl < 2; ++lvl)
       if ((rc = dalloc(e, &e->psiH[lvl][q], eH[q] * S))) return rc;
@@ -1001,6 +1004,92 @@ int pf_read_flux(pf_engine* e, int mon, double* dst) {
   if (rc) return rc;
   PF_CUDA(e, cudaMemcpyAsync(dst, e->fluxes[mon].acc, 8, cudaMemcpyDeviceToHost, e->stream));
   PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  return PF_OK;
+}
+
+int pf_write_field(pf_engine* e, int comp, const void* src) {
+  if (!e || !src) return PF_ERR_INVALID;
+  if (!e->finalized) return fail(e, PF_ERR_STATE, "pf_write_field before pf_finalize");
+  if (!valid_comp(comp)) return fail(e, PF_ERR_INVALID, "bad component %d", comp);
+  PF_CUDA(e, cudaSetDevice(e->device));
+  void* dst = comp < 3 ? e->E[e->cur][comp] : e->H[e->cur][comp - 3];
+  PF_CUDA(e, cudaMemcpyAsync(dst, src, (size_t)e->ncell * e->rb, cudaMemcpyHostToDevice, e->stream));
+  PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  return PF_OK;
+}
+
+namespace {
+// The stepping state as a list of (device pointer, bytes) pieces in the
+// order of the state blob: the six current field components, the six E psi
+// arrays, the six current H psi arrays, then the polarisation level holding
+// P^n followed by the one holding P^(n-1) for `step` n.
+std::vector<std::pair<char*, size_t>> state_pieces(pf_engine* e, long long step) {
+  std::vector<std::pair<char*, size_t>> v;
+  const size_t S = e->rb, n = (size_t)e->ncell * S;
+  for (int c = 0; c < 3; ++c) v.push_back({(char*)e->E[e->cur][c], n});
+  for (int c = 0; c < 3; ++c) v.push_back({(char*)e->H[e->cur][c], n});
+  for (int q = 0; q < 6; ++q) v.push_back({(char*)e->psiE[q], (size_t)e->npsiE[q] * S});
+  for (int q = 0; q < 6; ++q) v.push_back({(char*)e->psiH[e->cur][q], (size_t)e->npsiH[q] * S});
+  if (e->n_media > 0) {
+    const size_t lev = (size_t)e->plev * S;
+    const int ln = (int)(step & 1);
+    v.push_back({(char*)e->P + ln * lev, lev});
+    v.push_back({(char*)e->P + (ln ^ 1) * lev, lev});
+  }
+  return v;
+}
+
+int copy_state(pf_engine* e, long long step, void* buf, int64_t bytes, int on_device, bool get) {
+  if (!e || !buf) return PF_ERR_INVALID;
+  if (!e->finalized) return fail(e, PF_ERR_STATE, "state access before pf_finalize");
+  const auto pieces = state_pieces(e, step);
+  size_t total = 0;
+  for (const auto& p : pieces) total += p.second;
+  if ((int64_t)total != bytes)
+    return fail(e, PF_ERR_INVALID, "state buffer holds %lld bytes, the state is %zu",
+                (long long)bytes, total);
+  PF_CUDA(e, cudaSetDevice(e->device));
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice
+                                        : (get ? cudaMemcpyDeviceToHost : cudaMemcpyHostToDevice);
+  size_t off = 0;
+  for (const auto& p : pieces) {
+    if (p.second) {
+      char* b = (char*)buf + off;
+      if (get) PF_CUDA(e, cudaMemcpyAsync(b, p.first, p.second, kind, e->stream));
+      else PF_CUDA(e, cudaMemcpyAsync(p.first, b, p.second, kind, e->stream));
+    }
+    off += p.second;
+  }
+  PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  return PF_OK;
+}
+}  // namespace
+
+int pf_state_bytes(const pf_engine* e, int64_t* bytes) {
+  if (!e || !bytes) return PF_ERR_INVALID;
+  if (!e->finalized) return PF_ERR_STATE;
+  size_t total = 0;
+  for (const auto& p : state_pieces(const_cast<pf_engine*>(e), e->step)) total += p.second;
+  *bytes = (int64_t)total;
+  return PF_OK;
+}
+
+int pf_get_state(pf_engine* e, void* dst, int64_t bytes, int dst_on_device) {
+  if (!e) return PF_ERR_INVALID;
+  return copy_state(e, e->step, dst, bytes, dst_on_device, true);
+}
+
+int pf_set_state(pf_engine* e, int64_t step, const void* src, int64_t bytes, int src_on_device) {
+  if (!e) return PF_ERR_INVALID;
+  if (!e->finalized) return fail(e, PF_ERR_STATE, "pf_set_state before pf_finalize");
+  if (step < 0 || step > e->n_steps)
+    return fail(e, PF_ERR_INVALID, "step %lld outside [0, n_steps]", (long long)step);
+  // samples already taken belong to the old timeline: fold them first
+  int rc = e->rb == 4 ? flush_monitors<float>(e) : flush_monitors<double>(e);
+  if (rc) return rc;
+  rc = copy_state(e, step, const_cast<void*>(src), bytes, src_on_device, false);
+  if (rc) return rc;
+  e->step = step;
   return PF_OK;
 }
 

@@ -31,10 +31,13 @@ static __device__ __align__(256) double g_flux_partials[kNoAllocBlocks];
 
 // Device address of g_flux_partials per device. In host code the array's
 // name is only a host-side stand-in, so kernels always get this address.
+// It is looked up again on every call made outside a stream capture (the
+// lookup allocates nothing), so a module reloaded after cudaDeviceReset is
+// followed; a capture uses the address the last uncaptured call on that
+// device found. A failed lookup is never kept.
 constexpr int kMaxDevices = 64;
 double* g_partials_ptr[kMaxDevices];
-cudaError_t g_setup_rc[kMaxDevices];
-std::once_flag g_setup_once[kMaxDevices];
+std::mutex g_ptr_mutex;
 thread_local char g_err[256];
 
 // Per-block partial sums of S = E_t1*H_t2 - E_t2*H_t1 over the plane, with
@@ -118,15 +121,26 @@ int pf_flux_plane_noalloc(int real_bytes, int nx, int ny, int nz, const void* co
   cudaError_t rc = cudaGetDevice(&dev);
   if (rc != cudaSuccess) return set_error(PF_ERR_CUDA, cudaGetErrorString(rc));
   if (dev < 0 || dev >= kMaxDevices) return set_error(PF_ERR_UNSUPPORTED, "device index too large");
-  // First call on this device: resolve the scratch array's device address
-  // with the device current.
-  std::call_once(g_setup_once[dev], [dev]() {
-    g_setup_rc[dev] = cudaGetSymbolAddress((void**)&g_partials_ptr[dev], g_flux_partials);
-  });
-  if (g_setup_rc[dev] != cudaSuccess)
-    return set_error(PF_ERR_CUDA, cudaGetErrorString(g_setup_rc[dev]));
-  double* part = g_partials_ptr[dev];
   cudaStream_t st = (cudaStream_t)stream;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  rc = cudaStreamIsCapturing(st, &cap);
+  if (rc != cudaSuccess) return set_error(PF_ERR_CUDA, cudaGetErrorString(rc));
+  double* part = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_ptr_mutex);
+    if (cap == cudaStreamCaptureStatusNone) {
+      // Resolve the scratch array's device address with the device current.
+      double* p_dev = nullptr;
+      rc = cudaGetSymbolAddress((void**)&p_dev, g_flux_partials);
+      if (rc != cudaSuccess) return set_error(PF_ERR_CUDA, cudaGetErrorString(rc));
+      g_partials_ptr[dev] = p_dev;
+    } else if (g_partials_ptr[dev] == nullptr) {
+      return set_error(PF_ERR_STATE,
+                       "first call on this device made during a stream capture: call once "
+                       "outside the capture first");
+    }
+    part = g_partials_ptr[dev];
+  }
   if (real_bytes == 4) {
     Fields6<float> f;
     for (int c = 0; c < 6; ++c) f.f[c] = (const float*)fields[c];

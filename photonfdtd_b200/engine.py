@@ -67,7 +67,7 @@ def _eps_dtype(sim):
     return np.dtype(sim.dtypes["eps_r"]).type
 
 
-def material_words(sim):
+def material_words(sim, edt=None):
     """Per-cell uint32 word in table mode, the table values, and ADE cells.
 
     Stamps value indices instead of permittivities in structure order
@@ -83,7 +83,7 @@ def material_words(sim):
     word = np.zeros(shape, dtype=np.uint32)
     med_ids = np.full(shape, -1, dtype=np.int16)
     media, med_index = [], {}
-    edt = _eps_dtype(sim)
+    edt = _eps_dtype(sim) if edt is None else edt
     for s in sim.structures:
         sel = _cells(s, grid)
         if sel is None:
@@ -174,33 +174,54 @@ def flux_plane(m, grid) -> Tuple[int, int, float]:
 # --------------------------------------------------------------------------- #
 # Tables
 # --------------------------------------------------------------------------- #
-def build_tables(sim) -> dict:
-    """Everything the engine consumes, in the forms the C ABI takes."""
+def _smoothed_components(sim, dtype):
+    """The subpixel tensor in `dtype`: the simulation's own components when
+    that is its working type, else recomputed (on the GPU for box scenes)."""
+    if np.dtype(dtype) == np.dtype(_eps_dtype(sim)):
+        return sim._smoothed_eps_components()
+    from .smoothing import device_available, smooth_permittivity, smooth_permittivity_device
+    if device_available():
+        try:
+            return smooth_permittivity_device(sim.grid, sim.structures, background_eps=1.0,
+                                              factor=sim.subpixel_factor, dtype=dtype)
+        except NotImplementedError:
+            pass
+    return smooth_permittivity(sim.grid, sim.structures, background_eps=1.0,
+                               factor=sim.subpixel_factor, dtype=dtype)
+
+
+def build_tables(sim, dtype=None) -> dict:
+    """Everything the engine consumes, in the forms the C ABI takes.
+
+    dtype (np.float32 / np.float64) overrides the simulation's working
+    precision: a float64 shadow of a float32 scene (the error statement of
+    photonfdtd_b200.accuracy) evaluates every table as a float64 run of the
+    same scene would."""
     grid = sim.grid
-    npdt = np.dtype(sim.dtypes["Ex"]).type
+    npdt = np.dtype(sim.dtypes["Ex"] if dtype is None else dtype).type
     dt, n_steps = float(sim.dt), int(sim.n_steps)
     t = dict(shape=tuple(grid.shape), npdt=npdt, dt=dt, n_steps=n_steps,
              dl=tuple(d if d > 0 else 1.0 for d in grid.cell_size),
              ch=float(npdt(dt / MU_0)))
     t["cpml"] = [tuple(np.ascontiguousarray(np.asarray(arr[a]), dtype=npdt)
                        for arr in (sim._b_e, sim._c_e, sim._b_h, sim._c_h)) for a in range(3)]
-    edt = _eps_dtype(sim)
+    edt = _eps_dtype(sim) if dtype is None else npdt
     custom = bool(getattr(sim, "_eps_r_custom", False))
     need_ids = getattr(sim, "_has_dispersion", False) or not (custom or sim.subpixel)
     word = vals = med_ids = None
     media: list = []
     if need_ids:
-        word, vals, med_ids, media = material_words(sim)
+        word, vals, med_ids, media = material_words(sim, edt)
     ade = ade_tables(sim, med_ids, media, dt) if media else None
     if ade is not None and not ade["media"]:
         ade = None
     if sim.subpixel and not custom:
-        comps = sim._smoothed_eps_components()
+        comps = _smoothed_components(sim, edt)
         t["ce_mode"] = N.PF_CE_CELL3
         t["ce"] = [np.ascontiguousarray((dt / (np.asarray(e) * EPS_0)).astype(edt, copy=False),
                                         dtype=npdt) for e in comps]
     elif custom:
-        eps = np.asarray(sim.eps_r)
+        eps = np.asarray(sim.eps_r).astype(edt, copy=False)
         t["ce_mode"] = N.PF_CE_CELL1
         t["ce"] = [np.ascontiguousarray((dt / (eps * EPS_0)).astype(edt, copy=False),
                                         dtype=npdt)]
@@ -377,6 +398,38 @@ class B200Engine:
             self._cache[comp] = out
         return self._cache[comp]
 
+    def set_field(self, comp: str, arr: np.ndarray) -> None:
+        """Overwrite one component of the current state (pf_write_field)."""
+        src = np.ascontiguousarray(arr, dtype=self.npdt)
+        if src.shape != tuple(self.shape):
+            raise ValueError(f"field of shape {src.shape}, the grid is {self.shape}")
+        self._cache.clear()
+        self._chk(self._L.pf_write_field(self.h, _COMP[comp], N.ptr(src)))
+
+    def state_bytes(self) -> int:
+        import ctypes as C
+        v = C.c_int64()
+        self._chk(self._L.pf_state_bytes(self.h, C.byref(v)))
+        return int(v.value)
+
+    def get_state(self) -> np.ndarray:
+        """The stepping state blob (fields, psi, polarisation) as bytes."""
+        out = np.empty(self.state_bytes(), dtype=np.uint8)
+        self._chk(self._L.pf_get_state(self.h, N.ptr(out), out.size, 0))
+        return out
+
+    def set_state(self, step: int, blob: np.ndarray) -> None:
+        """Restore a blob from get_state and set the step counter."""
+        b = np.ascontiguousarray(blob, dtype=np.uint8)
+        self._cache.clear()
+        self._chk(self._L.pf_set_state(self.h, int(step), N.ptr(b), b.size, 0))
+
+    def step(self) -> int:
+        import ctypes as C
+        v = C.c_int64()
+        self._chk(self._L.pf_step(self.h, C.byref(v)))
+        return int(v.value)
+
     def read_dft(self, k: int, comp: str, n_freq: int, counts) -> np.ndarray:
         import ctypes as C
         out = np.empty((n_freq,) + tuple(counts), dtype=np.complex128)
@@ -461,20 +514,72 @@ def _result_cls(sim):
 
 
 def run_b200(sim, kernel: int = N.PF_KERNEL_AUTO):
-    """Run ``sim`` on the B200 engine and return a Result."""
+    """Run ``sim`` on the B200 engine and return a Result.
+
+    With ``sim.b200_error_vs_f64 = True`` on a float32 scene, the Result also
+    carries ``error_vs_f64``: every output's error against a float64 run of
+    the same scene on the engine (photonfdtd_b200.accuracy), whose float64
+    arithmetic reproduces the reference's float64 NumPy run to 1e-12."""
+    import time
+    t0 = time.perf_counter()
     validate(sim)
     t = build_tables(sim)
+    t1 = time.perf_counter()
     eng = B200Engine(t, kernel=kernel)
+    t2 = time.perf_counter()
     try:
-        return drive(sim, eng, t)
+        res = drive(sim, eng, t)
     finally:
         eng.close()
+    t3 = time.perf_counter()
+    LAST_RUN.clear()
+    LAST_RUN.update(tables_s=t1 - t0, create_s=t2 - t1, run_s=t3 - t2,
+                    h2d_bytes=upload_bytes(t), n_steps=t["n_steps"],
+                    d2h_bytes=result_bytes(res), cells=int(np.prod(t["shape"])))
+    if getattr(sim, "b200_error_vs_f64", False) and np.dtype(t["npdt"]) != np.float64:
+        from .accuracy import error_vs_f64, float64_shadow
+        res.error_vs_f64 = error_vs_f64(res, float64_shadow(sim, kernel))
+    return res
 
 
-def drive(sim, eng: B200Engine, t: dict):
+# Phase timings and transfer sizes of the last run_b200 call (seconds, bytes):
+# building the tables on the host, creating the engine (device allocation and
+# upload), stepping with monitor read-back.
+LAST_RUN: Dict[str, float] = {}
+
+
+def upload_bytes(t) -> int:
+    """Host-to-device bytes of an engine's tables."""
+    n = 0
+    if t["ce_mode"] == N.PF_CE_TABLE:
+        n += t["word"].nbytes + t["table"].nbytes
+    else:
+        n += sum(a.nbytes for a in t["ce"])
+    for ax in t["cpml"]:
+        n += sum(a.nbytes for a in ax)
+    if t["ade"] is not None and t["ade"]["cell_word"] is not None:
+        n += t["ade"]["cell_word"].nbytes
+    s = t["sources"]
+    n += s["wave"].nbytes + s["amp"].nbytes + s["cell"].nbytes
+    for d in t["dft"]:
+        n += d["ph_e"].nbytes + d["ph_h"].nbytes
+    return int(n)
+
+
+def result_bytes(res) -> int:
+    """Device-to-host bytes of a Result's monitor data."""
+    n = 0
+    for comps in res.fields.values():
+        n += sum(np.asarray(a).nbytes for a in comps.values())
+    for comps in res.dft.values():
+        n += sum(np.asarray(a).nbytes for a in comps.values())
+    return int(n + 8 * len(res.flux))
+
+
+def drive(sim, eng: B200Engine, t: dict, mon_dtype=None):
     grid = sim.grid
     dt, n_steps = t["dt"], t["n_steps"]
-    mon_dtype = sim.dtypes["monitors"]
+    mon_dtype = sim.dtypes["monitors"] if mon_dtype is None else mon_dtype
     Result = _result_cls(sim)
     result = Result(times=np.arange(n_steps) * dt)
     rec: Dict[str, dict] = {}

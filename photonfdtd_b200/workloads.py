@@ -110,11 +110,46 @@ def config3_plain_media(pf):
     return tuple(pf.Medium(permittivity=e) for e in (1.0, 4.0, 2.1))
 
 
+class BlockMedium:
+    """All blocks of one medium in a block-structured scene, as one structure.
+
+    It follows the reference's structure protocol (src/photonfdtd/geometry.py
+    Box.region_mask / Box.stamp): ``region_mask(grid)`` is the boolean grid
+    of the medium's cells, ``stamp(grid, eps_r)`` writes its permittivity
+    there, ``medium`` is the medium. The blocks of different media are
+    disjoint, so one such structure per medium rasterises to exactly the
+    cells (and ADE media) that one Box per block gives; it only spares a
+    rasteriser that walks the full grid per structure (the reference's) one
+    pass per block."""
+
+    def __init__(self, medium, ids: np.ndarray, which: int, block: int):
+        self.medium = medium
+        self._ids = ids
+        self._which = which
+        self._block = block
+
+    def region_mask(self, grid) -> np.ndarray:
+        b = self._block
+        m = (self._ids == self._which).repeat(b, 0).repeat(b, 1).repeat(b, 2)
+        shape = tuple(grid.shape)
+        out = np.zeros(shape, dtype=bool)
+        n = [min(shape[a], m.shape[a]) for a in range(3)]
+        out[:n[0], :n[1], :n[2]] = m[:n[0], :n[1], :n[2]]
+        return out
+
+    def stamp(self, grid, eps_r: np.ndarray) -> None:
+        eps_r[self.region_mask(grid)] = self.medium.eps_r
+
+
 def config3(pf, n_total: int = 384, block: int = 8, n_steps: int = 3000,
             flux: bool = True, dft: bool = True, precision: str = "float32",
-            flux_pos: float = None, dispersive: bool = True):
+            flux_pos: float = None, dispersive: bool = True, union_blocks: bool = False,
+            **sim_kw):
     """3D dispersive ADE mix in 8^3 blocks, six flux planes, a z-plane DFT.
-    dispersive=False swaps in config3_plain_media (same grid and blocks)."""
+    dispersive=False swaps in config3_plain_media (same grid and blocks).
+    union_blocks=True describes the blocks as one BlockMedium per medium
+    instead of one Box per block (same cells, same media). sim_kw go to the
+    Simulation (e.g. the reference's use_numba or backend)."""
     d = 10e-9
     grid = pf.Grid(size=(n_total * d,) * 3, cell_size=d, pml_layers=12)
     media = config3_media(pf) if dispersive else config3_plain_media(pf)
@@ -122,14 +157,18 @@ def config3(pf, n_total: int = 384, block: int = 8, n_steps: int = 3000,
     ids = config3_block_ids(nb)
     x0 = -(n_total - 1) / 2 * d            # coordinate of cell 0
     boxes = []
-    for bi in range(nb):
-        for bj in range(nb):
-            for bk in range(nb):
-                # box spanning cells [b*block, (b+1)*block) on each axis: its
-                # faces sit half a cell outside the first and last centres.
-                c = [x0 + (b * block + (block - 1) / 2) * d for b in (bi, bj, bk)]
-                boxes.append(pf.Box(center=tuple(c), size=(block * d,) * 3,
-                                    medium=media[int(ids[bi, bj, bk])]))
+    if union_blocks:
+        boxes = [BlockMedium(media[q], ids, q, block) for q in range(3)]
+    else:
+        for bi in range(nb):
+            for bj in range(nb):
+                for bk in range(nb):
+                    # box spanning cells [b*block, (b+1)*block) on each axis:
+                    # its faces sit half a cell outside the first and last
+                    # centres.
+                    c = [x0 + (b * block + (block - 1) / 2) * d for b in (bi, bj, bk)]
+                    boxes.append(pf.Box(center=tuple(c), size=(block * d,) * 3,
+                                        medium=media[int(ids[bi, bj, bk])]))
     src = pf.PointDipole(position=(0.0, 0.0, 0.0), component="Ex",
                          waveform=pf.GaussianPulse(freq0=C_0 / 0.8e-6, fwhm=10e-15))
     mons = []
@@ -145,7 +184,7 @@ def config3(pf, n_total: int = 384, block: int = 8, n_steps: int = 3000,
                                   plane_axis="z", plane_position=0.0))
     dt = _dt(d, 3)
     return pf.Simulation(grid, structures=boxes, sources=[src], monitors=mons,
-                         run_time=_run_time_for(n_steps, dt), precision=precision)
+                         run_time=_run_time_for(n_steps, dt), precision=precision, **sim_kw)
 
 
 # --------------------------------------------------------------------------- #

@@ -1,9 +1,11 @@
 """Write the golden fixtures: outputs of the reference photonfdtd itself.
 
-Run in a container where the reference source tree is present (it is read,
-never modified):
+Run where the reference package is importable: installed in baseline/_ref
+(python -m baseline.install_ref) or found as a source tree by
+baseline.locate (PHOTONFDTD_REFERENCE, or a ``reference`` directory beside
+the repository). The reference is read, never modified:
 
-    PYTHONPATH=/root/reference/src python tests/golden/make_golden.py [names...]
+    python tests/golden/make_golden.py [names...]
 
 Each scene of ``tests/scenes.py`` is built against the reference package,
 run with ``backend="numpy"`` (the reference's vectorised float32/float64
@@ -30,8 +32,12 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
 sys.path.insert(0, os.path.dirname(HERE))
 
-import photonfdtd as ref  # noqa: E402  (reference, from PYTHONPATH)
+from baseline.locate import import_reference  # noqa: E402
 import scenes  # noqa: E402
+
+ref = import_reference()
+if ref is None:
+    raise SystemExit("the reference photonfdtd package is not importable here")
 
 # Frames kept per FieldMonitor when a scene records many.
 MAX_FRAMES = 6
@@ -58,14 +64,19 @@ def run_scene(name):
         for c, arr in comps.items():
             out[f"f/{mon}/{c}"] = np.asarray(arr)[k]
         out[f"ft/{mon}"] = np.asarray(res.monitor_times[mon])
+    thin = scenes.THIN_DFT.get(name)
     for mon, comps in res.dft.items():
         for c, arr in comps.items():
+            if thin is not None:
+                if c not in thin["comps"]:
+                    continue
+                arr = np.asarray(arr)[list(thin["freqs"])]
             out[f"dft/{mon}/{c}"] = np.asarray(arr)
         out[f"dftf/{mon}"] = np.asarray(res.dft_freqs[mon])
     for mon, v in res.flux.items():
         out[f"flux/{mon}"] = np.float64(v)
     meta = dict(scene=name, dt=sim.dt, n_steps=sim.n_steps, wall_s=wall,
-                keep=keep, numpy=np.__version__, reference=ref.__version__,
+                keep=keep, thin_dft=thin, numpy=np.__version__, reference=ref.__version__,
                 shape=list(sim.grid.shape))
     out["meta"] = np.array(json.dumps(meta))
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)

@@ -21,7 +21,8 @@ def compare(res, name):
     """Relative max-abs and relative L2 differences of every golden array.
 
     Returns {key: (rel_max, rel_l2)} with both scaled by the golden array's
-    max |value| / L2 norm."""
+    max |value| / L2 norm. A fixture whose DFT was thinned (meta
+    "thin_dft") is compared on the frequencies it kept."""
     g, meta = load(name)
     out = {}
     for k in g.files:
@@ -31,6 +32,9 @@ def compare(res, name):
         elif k.startswith("dft/"):
             _, mon, c = k.split("/")
             a = np.asarray(_get(res, "dft", mon, c))
+            thin = meta.get("thin_dft")
+            if thin is not None:
+                a = a[list(thin["freqs"])]
         elif k.startswith("flux/"):
             a = np.asarray(_get(res, "flux", k.split("/")[1]))
         else:

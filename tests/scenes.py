@@ -130,6 +130,20 @@ def ade3d(pf, precision="float32", n_steps=3000):
     return sim
 
 
+def c2rep(pf, precision="float32", n_steps=2000):
+    """Config-2 replica at reduced size: a 96^3 interior (120^3 grid with the
+    12-cell CPML) at 20 nm, 8 seeded boxes with centres and sides scaled by
+    96/512, subpixel smoothing (factor 3), the Ex dipole and the 16-wavelength
+    DFT on the z = 0 plane, over the full 2000 steps; plus the six fields on
+    that plane at step 700 (pulse inside the domain) and at the last step (a
+    residual of about 1e-8 of the peak, dominated by round-off)."""
+    sim = W.config2(pf, interior=96, n_boxes=8, n_freqs=16, n_steps=n_steps,
+                    subpixel=True, precision=precision)
+    sim.add_monitor(pf.FieldMonitor(name="mid", components=ALL6, plane_z=0.0,
+                                    times=[700 * sim.dt, (n_steps - 1) * sim.dt]))
+    return sim
+
+
 def te2d(pf, precision="float32", n_steps=2000):
     """Reduced config-4 recipe: one 120 x 90 instance, 32 x 32 design."""
     rho = W.config4_density(7, design=32)
@@ -154,6 +168,20 @@ SCENES = {
     "sub3d_f32": (sub3d, dict(precision="float32")),
     "ade3d_f32": (ade3d, dict(precision="float32")),
     "te2d_f32": (te2d, dict(precision="float32")),
+    # float64 runs of the reduced config-2/3/4 recipes: the float32 runs'
+    # error against them is what every float32 result states
+    "sub3d_f64": (sub3d, dict(precision="float64")),
+    "ade3d_f64": (ade3d, dict(precision="float64")),
+    "te2d_f64": (te2d, dict(precision="float64")),
+    "c2rep_f32": (c2rep, dict(precision="float32")),
+    "c2rep_f64": (c2rep, dict(precision="float64")),
+}
+
+# DFT results thinned in the fixtures (frequency indices and components
+# kept), to keep them small; tests slice their own runs the same way.
+THIN_DFT = {
+    "c2rep_f32": dict(freqs=(0, 7, 15), comps=("Ex", "Hy")),
+    "c2rep_f64": dict(freqs=(0, 7, 15), comps=("Ex", "Hy")),
 }
 
 

@@ -27,8 +27,16 @@ def _rank(rank, world, port, out):
         dist.destroy_process_group()
 
 
+def free_port() -> int:
+    """A TCP port on 127.0.0.1 that nothing listens on (the OS picks it)."""
+    import socket
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
 def test_two_ranks_report_the_slowest_time_and_the_job_rate():
-    port = 29500 + os.getpid() % 1000
+    port = free_port()
     with mp.Manager() as m:
         out = m.dict()
         mp.spawn(_rank, args=(2, port, out), nprocs=2, join=True)

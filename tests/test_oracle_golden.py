@@ -13,7 +13,11 @@ import scenes
 from golden_util import compare, load
 from oracle import run_oracle
 
-FAST = [n for n in scenes.SCENES if n not in ("ade3d_f32",)]
+# the 3000-step ADE scenes take ~90 s each here (one is pinned by the slow
+# test below); the 120^3 config-2 replicas take minutes and are pinned on the
+# GPU against the same fixtures
+FAST = [n for n in scenes.SCENES
+        if n not in ("ade3d_f32", "ade3d_f64", "c2rep_f32", "c2rep_f64")]
 
 
 @pytest.mark.parametrize("name", FAST)

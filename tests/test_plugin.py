@@ -1,24 +1,21 @@
 """The plugin registers backend="b200" on the reference photonfdtd package.
 
-Runs only where the reference is importable (the build container); the
-engine call itself is replaced by a recorder, so no GPU is needed.
+Runs where the reference is importable (its copy installed in baseline/_ref,
+or its source tree); the engine call itself is replaced by a recorder, so no
+GPU is needed.
 """
 import os
 import sys
 
 import pytest
 
-REF = "/root/reference/src"
-
 
 def _reference():
-    if os.path.isdir(REF) and REF not in sys.path:
-        sys.path.append(REF)
-    try:
-        import photonfdtd
-    except ImportError:
+    from baseline.locate import import_reference
+    ref = import_reference()
+    if ref is None:
         pytest.skip("reference package not importable here")
-    return photonfdtd
+    return ref
 
 
 def test_install_routes_b200_runs(monkeypatch):

@@ -7,13 +7,16 @@ pf_flux_plane_noalloc serves them: it computes one step's flux contribution
 from caller-owned field buffers into a caller-owned device double, keeping
 its partial sums in a fixed device array instead of allocating scratch.
 
-Here the engine steps a small 3D scene with two flux monitors; after each of
-two consecutive steps the fields are copied into separate device buffers and
-the entry point is called on them, twice in a row per monitor. Summed onto
-the engine's earlier integral, the contributions must give the engine's own
-integral after those steps (the flux tolerance of the parity tests; the
-reduction order is the same, so the sums agree exactly). The file is named
-to run after every other GPU test and depends on no state they leave.
+Here the engine steps a small 3D scene with three flux monitors, one normal
+to each axis, so every plane-indexing branch of the entry point runs. On each
+of two consecutive steps the fields are copied into separate device buffers
+and the entry point is called once per monitor on them, so it is called
+twice in a row per monitor. Added onto the engine's integral from before
+those steps, in the order the engine adds its own per-step terms, the
+contributions must equal the engine's integral after them exactly: the
+partial sums use the same block layout, roundings and fold order as the
+engine's flux sampling, so no tolerance is needed. The file is named to run
+after every other GPU test and depends on no state they leave.
 """
 import ctypes as C
 
@@ -36,6 +39,7 @@ def _scene(precision):
     src = pf.PointDipole(position=(0.0, 0.0, 0.0), component="Ez",
                          waveform=pf.GaussianPulse(freq0=250e12, fwhm=4e-15))
     mons = [pf.FluxMonitor(name="fx", plane_axis="x", plane_position=0.0),
+            pf.FluxMonitor(name="fy", plane_axis="y", plane_position=-0.08e-6),
             pf.FluxMonitor(name="fz", plane_axis="z", plane_position=0.1e-6)]
     return pf.Simulation(grid, structures=[box], sources=[src], monitors=mons,
                          run_time=60e-15, precision=precision)
@@ -68,9 +72,10 @@ def test_noalloc_flux_matches_engine(precision):
         want = [eng.read_flux(k) for k in range(len(t["flux"]))]
     finally:
         eng.close()
+    assert sorted(f["axis"] for f in t["flux"]) == [0, 1, 2]
     for got, ref in zip(acc, want):
         assert ref != 0.0
-        assert abs(got - ref) <= 1e-6 * abs(ref), (got, ref)
+        assert got == ref, (got, ref)
 
 
 def test_noalloc_rejects_oversized_plane():
