@@ -147,6 +147,15 @@ int pf_advance(pf_engine *eng, int64_t step0, int64_t n_sub);
  * (rust/src/cuda.rs:552-564, read_field). */
 int pf_read_field(pf_engine *eng, int comp, void *host_dst);
 
+/* A strided sub-block of one current field component into host memory:
+ * cells start[a], start[a] + stride[a], ... < stop[a] on each axis, C order
+ * (the FieldMonitor snapshot of simulation.py:1062-1067: every downsample-th
+ * cell, or one plane_z plane). The gather runs on the device, so only the
+ * snapshot crosses to the host (the reference copies whole fields). The
+ * engine keeps a device staging buffer of the largest region read. */
+int pf_read_region(pf_engine *eng, int comp, const int32_t start[3],
+                   const int32_t stop[3], const int32_t stride[3], void *host_dst);
+
 /* DFT accumulator of monitor mon, component comp: n_freq x region cells
  * complex128 as interleaved (re, im) doubles (simulation.py:1124-1133). */
 int pf_read_dft(pf_engine *eng, int mon, int comp, double *host_dst);
@@ -181,6 +190,21 @@ int pf_step(const pf_engine *eng, int64_t *step);
 
 /* Scan all six fields for non-finite values: PF_OK or PF_ERR_NONFINITE. */
 int pf_check_finite(pf_engine *eng);
+
+/* Failure detection while stepping: with k > 0, pf_advance scans the fields
+ * after every step whose count is a multiple of k and stops there with
+ * PF_ERR_NONFINITE (the engine stays at that step) once a value is inf or
+ * nan, e.g. a run past its Courant limit. 0 (the default) turns it off. The
+ * reference has no such check. */
+int pf_set_check_every(pf_engine *eng, int64_t k);
+
+/* Test hook of the TMA-staged fused step (PF_KERNEL_FUSED where the grid
+ * allows TMA): with on != 0, block (0, 0, 0) of every step waits once on a
+ * barrier that nothing arrives on, with a short limit, so the wait runs out
+ * and the block takes its timeout path (it lets its issued copies land, sets
+ * the error flag and leaves); pf_advance then returns PF_ERR_TIMEOUT and the
+ * fields are invalid. No counterpart in the reference. */
+int pf_set_wait_test(pf_engine *eng, int on);
 
 /* The CUDA stream (a cudaStream_t) the engine launches on, so a caller can
  * time its work with events on that stream. */
@@ -342,7 +366,9 @@ int pfb_read_grad(pf_batch *b, double *dst);
 /* Component comp (0 Ex, 1 Ey, 2 Hz) of instance k, nx*ny reals. */
 int pfb_read_field(pf_batch *b, int k, int comp, void *dst);
 /* out[0..n_out): cells, line cells, design cells, tiles, K, segments,
- * reals per stored state, kernel launches issued so far. */
+ * reals per stored state, kernel launches issued so far, and 1 when the
+ * forward and reverse steps run as one fused launch each on double-buffered
+ * state (every batch without Hz sources), 0 for the split passes. */
 int pfb_info(const pf_batch *b, int64_t *out, int n_out);
 /* The batch's cudaStream_t. */
 void *pfb_stream(pf_batch *b);
@@ -378,6 +404,12 @@ int pfs_gemm_engine(int engine);
 /* Number of tcgen05 GEMM blocks whose bounded wait for their MMAs ran out
  * (their output tile is then not written); reset = 1 clears it. Synchronous. */
 int pfs_gemm_timeouts(int *count, int reset);
+/* Test hook of the tcgen05 GEMM for the process: with on = 1, the MMA warp of
+ * block (0, 0, 0) first waits 100 us on a barrier nothing arrives on, so the
+ * wait runs out and the block takes its timeout path (it drains its loads,
+ * counts a timeout, leaves its tile unwritten and frees its tensor memory).
+ * 0 turns it off; other values only query. Returns the previous setting. */
+int pfs_gemm_wait_test(int on);
 /* Lowering of a 2D convolution (kernel kh x kw, stride, zero padding ph
  * rows / pw columns) over NHWC BF16 input x (nb, H, W, C): col rows
  * (b, oy, ox), columns (ky * kw + kx) * C + c, zero-padded to Kp. */

@@ -60,6 +60,10 @@ SIGNATURES = {
     "pf_read_flux": (C.c_int, [_vp, C.c_int, _pdbl]),
     "pf_step": (C.c_int, [_vp, _pi64]),
     "pf_write_field": (C.c_int, [_vp, C.c_int, _vp]),
+    "pf_set_check_every": (C.c_int, [_vp, _i64]),
+    "pf_set_wait_test": (C.c_int, [_vp, C.c_int]),
+    "pf_read_region": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                 C.POINTER(C.c_int32), _vp]),
     "pf_state_bytes": (C.c_int, [_vp, _pi64]),
     "pf_get_state": (C.c_int, [_vp, _vp, _i64, C.c_int]),
     "pf_set_state": (C.c_int, [_vp, _i64, _vp, _i64, C.c_int]),
@@ -105,6 +109,7 @@ SIGNATURES = {
                                        _vp]),
     "pfs_gemm_engine": (C.c_int, [C.c_int]),
     "pfs_gemm_timeouts": (C.c_int, [C.POINTER(C.c_int), C.c_int]),
+    "pfs_gemm_wait_test": (C.c_int, [C.c_int]),
     "pfs_im2col": (C.c_int, [C.c_int] * 9 + [_vp, _vp, C.c_int, _vp]),
     "pfs_col2im": (C.c_int, [C.c_int] * 9 + [_vp, C.c_int, _vp, _vp]),
     "pfs_bias_act": (C.c_int, [_i64, C.c_int, _vp, _vp, C.c_int, _vp, _vp, _vp]),

@@ -366,10 +366,10 @@ class BatchTE:
         return out
 
     def info(self) -> dict:
-        v = (C.c_int64 * 8)()
-        self._chk(self._L.pfb_info(self.h, v, 8))
+        v = (C.c_int64 * 9)()
+        self._chk(self._L.pfb_info(self.h, v, 9))
         keys = ("cells", "line_cells", "design_cells", "tiles", "checkpoint_every",
-                "segments", "state_reals", "launches")
+                "segments", "state_reals", "launches", "fused")
         return dict(zip(keys, list(v)))
 
     def stream(self) -> int:

@@ -77,6 +77,13 @@ struct pf_batch {
   int tile_rows = 32;
   size_t tile_cap = 0;  // TileRec slots of d_tiles (the 8-row list, the longest)
   void *Ex = nullptr, *Ey = nullptr, *Hz = nullptr, *ce = nullptr;
+  // fused step (no H-family sources): a second level of Ex, Ey, Hz and the
+  // H psi; the fields after `field_step` steps are in level_at(field_step)
+  bool fused = false;
+  void* lvl1[5] = {};  // Ex, Ey, Hz, psi[0], psi[1] of level 1
+  long long field_step = 0;
+  // fused reverse step: level 1 of aHz, its two psi adjoints, gA and gB
+  void* alvl1[5] = {};
   void* coef[8] = {};
   void* psi[4] = {};
   int* maps[4] = {};  // mex mhx mey mhy
@@ -174,8 +181,29 @@ BArgs<T> bargs(pf_batch* b) {
   a.ring = (T*)b->ring;
   a.n_design = b->n_design;
   a.ring_len = b->fwd_only ? 1 : b->ckpt;
+  T** lv[5] = {a.Ex2, a.Ey2, a.Hz2, a.pHzx2, a.pHzy2};
+  void* l0[5] = {b->Ex, b->Ey, b->Hz, b->psi[0], b->psi[1]};
+  for (int q = 0; q < 5; ++q) {
+    lv[q][0] = (T*)l0[q];
+    lv[q][1] = (T*)(b->fused ? b->lvl1[q] : l0[q]);
+  }
   return a;
 }
+
+template <typename T>
+BFields<T> bfields(const BArgs<T>& a, bool flip) {
+  BFields<T> f;
+  for (int l = 0; l < 2; ++l) {
+    f.Ex[l] = a.Ex2[l];
+    f.Ey[l] = a.Ey2[l];
+    f.Hz[l] = a.Hz2[l];
+  }
+  f.flip = flip ? 1 : 0;
+  return f;
+}
+
+// Level holding the fields after `step` steps (always 0 on the split path).
+int level_at(const pf_batch* b, long long step) { return b->fused ? (int)(step & 1) : 0; }
 
 template <typename T>
 AArgs<T> aargs(pf_batch* b) {
@@ -196,6 +224,12 @@ AArgs<T> aargs(pf_batch* b) {
   d.phase = b->phase;
   d.n_freq = b->n_freq;
   d.dt = b->dt;
+  T** lv[5] = {d.aHz2, d.aHzx2, d.aHzy2, d.gA2, d.gB2};
+  void* l0[5] = {b->aE[2], b->apsi[0], b->apsi[1], b->g[0], b->g[1]};
+  for (int q = 0; q < 5; ++q) {
+    lv[q][0] = (T*)l0[q];
+    lv[q][1] = (T*)(b->fused ? b->alvl1[q] : l0[q]);
+  }
   return d;
 }
 
@@ -205,37 +239,43 @@ int grid_blocks(const pf_batch* b) { return std::max(1, b->ntiles); }
 template <typename T, int R>
 void fwd_kernels(pf_batch* b, long long len, bool dft) {
   const BArgs<T> a = bargs<T>(b);
+  const BFields<T> f = bfields<T>(a, b->fused);
   const dim3 blk(32, kWarps);
   const int G = grid_blocks(b);
   const long long ng = b->src.n_groups;
   int pend = 0;
   for (long long t = 0; t < len; ++t) {
-    if (b->n_h_groups) {
-      kb_post<T><<<(unsigned)((ng + 127) / 128), 128, 0, b->stream>>>(
-          b->src, a.Ex, a.Ey, a.Hz, 1, b->base, (int)t, b->lcell, 0, (T*)nullptr);
-      ++b->capture_launches;
+    if (b->fused) {
+      kb_step<T, R><<<G, blk, 0, b->stream>>>(a, (int)t);
+      b->capture_launches += 1;
+    } else {
+      if (b->n_h_groups) {
+        kb_post<T><<<(unsigned)((ng + 127) / 128), 128, 0, b->stream>>>(
+            b->src, f, 1, b->base, (int)t, b->lcell, 0, (T*)nullptr);
+        ++b->capture_launches;
+      }
+      kb_h<T, R><<<G, blk, 0, b->stream>>>(a);
+      kb_e<T, R><<<G, blk, 0, b->stream>>>(a, (int)t);
+      b->capture_launches += 2;
     }
-    kb_h<T, R><<<G, blk, 0, b->stream>>>(a);
-    kb_e<T, R><<<G, blk, 0, b->stream>>>(a, (int)t);
-    b->capture_launches += 2;
     T* dring = dft ? (T*)b->dring : nullptr;
     if (b->merge_post || !dft) {
       const long long n = ng + (dft ? b->nline : 0);
       if (n) {
         kb_post<T><<<(unsigned)((n + 127) / 128), 128, 0, b->stream>>>(
-            b->src, a.Ex, a.Ey, a.Hz, 0, b->base, (int)t, b->lcell, b->nline, dring);
+            b->src, f, 0, b->base, (int)t, b->lcell, b->nline, dring);
         ++b->capture_launches;
       }
     } else {
       if (ng) {
         kb_post<T><<<(unsigned)((ng + 127) / 128), 128, 0, b->stream>>>(
-            b->src, a.Ex, a.Ey, a.Hz, 0, b->base, (int)t, b->lcell, 0, (T*)nullptr);
+            b->src, f, 0, b->base, (int)t, b->lcell, 0, (T*)nullptr);
         ++b->capture_launches;
       }
       BSources none = b->src;
       none.n_groups = 0;
       kb_post<T><<<(unsigned)((b->nline + 127) / 128), 128, 0, b->stream>>>(
-          none, a.Ex, a.Ey, a.Hz, 0, b->base, (int)t, b->lcell, b->nline, dring);
+          none, f, 0, b->base, (int)t, b->lcell, b->nline, dring);
       ++b->capture_launches;
     }
     if (dft) {
@@ -263,6 +303,17 @@ void adj_kernels(pf_batch* b, long long len) {
   const AArgs<T> d = aargs<T>(b);
   const dim3 blk(32, kWarps);
   const int G = grid_blocks(b);
+  if (b->fused) {
+    kb_adj_step<T, R, false, true><<<G, blk, 0, b->stream>>>(a, d, (int)(len - 1));
+    for (long long t = len - 1; t >= 0; --t) {
+      if (t > 0)
+        kb_adj_step<T, R, true, true><<<G, blk, 0, b->stream>>>(a, d, (int)t);
+      else
+        kb_adj_step<T, R, true, false><<<G, blk, 0, b->stream>>>(a, d, 0);
+    }
+    b->capture_launches += 1 + len;
+    return;
+  }
   kb_adj_cell<T, R, false, true><<<G, blk, 0, b->stream>>>(a, d, (int)(len - 1));
   for (long long t = len - 1; t >= 0; --t) {
     kb_adj_h<T, R><<<G, blk, 0, b->stream>>>(a, d);
@@ -315,11 +366,15 @@ int run_chunk(pf_batch* b, int kind, long long len) {
   return PF_OK;
 }
 
-// Copies the stepping state (Ex, Ey, Hz, four psi arrays) to / from slot s.
-int state_copy(pf_batch* b, long long s, bool save) {
+// Copies the stepping state (Ex, Ey, Hz, four psi arrays) to / from slot s;
+// `step` is the step count the state belongs to (it selects the level).
+int state_copy(pf_batch* b, long long s, bool save, long long step) {
   const size_t S = b->rb;
   char* base = (char*)b->ckpt_buf + (size_t)s * b->state_elems * S;
-  void* parts[7] = {b->Ex, b->Ey, b->Hz, b->psi[0], b->psi[1], b->psi[2], b->psi[3]};
+  const bool l1 = level_at(b, step) == 1;
+  void* parts[7] = {l1 ? b->lvl1[0] : b->Ex, l1 ? b->lvl1[1] : b->Ey, l1 ? b->lvl1[2] : b->Hz,
+                    l1 ? b->lvl1[3] : b->psi[0], l1 ? b->lvl1[4] : b->psi[1], b->psi[2],
+                    b->psi[3]};
   const long long n[7] = {b->ncell, b->ncell, b->ncell, b->npsi[0], b->npsi[1], b->npsi[2], b->npsi[3]};
   size_t o = 0;
   for (int q = 0; q < 7; ++q) {
@@ -346,6 +401,12 @@ int zero_state(pf_batch* b) {
   for (void* p : {b->Ex, b->Ey, b->Hz}) B_CUDA(b, cudaMemsetAsync(p, 0, b->ncell * S, b->stream));
   for (int q = 0; q < 4; ++q)
     if (b->npsi[q]) B_CUDA(b, cudaMemsetAsync(b->psi[q], 0, b->npsi[q] * S, b->stream));
+  if (b->fused) {
+    for (int q = 0; q < 3; ++q) B_CUDA(b, cudaMemsetAsync(b->lvl1[q], 0, b->ncell * S, b->stream));
+    for (int q = 0; q < 2; ++q)
+      if (b->npsi[q]) B_CUDA(b, cudaMemsetAsync(b->lvl1[3 + q], 0, b->npsi[q] * S, b->stream));
+  }
+  b->field_step = 0;
   return PF_OK;
 }
 
@@ -356,13 +417,14 @@ int forward_t(pf_batch* b) {
   B_CUDA(b, cudaMemsetAsync(b->acc, 0, (size_t)b->nline * b->n_freq * 16, b->stream));
   const long long K = b->ckpt;
   for (long long s0 = 0; s0 < b->n_steps; s0 += K) {
-    if (s0 > 0 && !b->fwd_only && (rc = state_copy(b, s0 / K - 1, true)))
+    if (s0 > 0 && !b->fwd_only && (rc = state_copy(b, s0 / K - 1, true, s0)))
       return rc;  // segment 0 starts at zero
     if ((rc = set_base(b, s0))) return rc;
     if ((rc = run_chunk<T>(b, 0, std::min(K, b->n_steps - s0)))) return rc;
   }
   B_CUDA(b, cudaGetLastError());
   B_CUDA(b, cudaStreamSynchronize(b->stream));
+  b->field_step = b->n_steps;
   b->fwd_done = true;
   b->ring_last = true;
   return PF_OK;
@@ -375,7 +437,12 @@ int adjoint_t(pf_batch* b) {
   for (int q = 0; q < 3; ++q) B_CUDA(b, cudaMemsetAsync(b->aE[q], 0, b->ncell * S, b->stream));
   for (int q = 0; q < 4; ++q) {
     if (b->npsi[q]) B_CUDA(b, cudaMemsetAsync(b->apsi[q], 0, b->npsi[q] * S, b->stream));
-    B_CUDA(b, cudaMemsetAsync(b->g[q], 0, b->ncell * S, b->stream));
+    if (q < 2 || !b->fused) B_CUDA(b, cudaMemsetAsync(b->g[q], 0, b->ncell * S, b->stream));
+  }
+  if (b->fused) {
+    const long long n1[5] = {b->ncell, b->npsi[0], b->npsi[1], b->ncell, b->ncell};
+    for (int q = 0; q < 5; ++q)
+      if (n1[q]) B_CUDA(b, cudaMemsetAsync(b->alvl1[q], 0, n1[q] * S, b->stream));
   }
   B_CUDA(b, cudaMemsetAsync(b->grad, 0, (size_t)b->n_design * 8, b->stream));
   const long long K = b->ckpt;
@@ -385,11 +452,12 @@ int adjoint_t(pf_batch* b) {
     if (sg < nseg - 1 || !b->ring_last) {  // refill the ring from the segment's checkpoint
       if (sg == 0) {
         if ((rc = zero_state(b))) return rc;
-      } else if ((rc = state_copy(b, sg - 1, false))) {
+      } else if ((rc = state_copy(b, sg - 1, false, s0))) {
         return rc;
       }
       if ((rc = set_base(b, s0))) return rc;
       if ((rc = run_chunk<T>(b, 1, len))) return rc;
+      b->field_step = s0 + len;
     }
     if ((rc = set_base(b, s0))) return rc;
     if ((rc = run_chunk<T>(b, 2, len))) return rc;
@@ -715,12 +783,31 @@ int pfb_finalize(pf_batch* b, int checkpoint_every, int tile_rows) {
     if ((rc = balloc(b, p, b->ncell * S))) return rc;
   for (int q = 0; q < 4; ++q)
     if ((rc = balloc(b, &b->psi[q], b->npsi[q] * S))) return rc;
+  // the fused steps need no H-family source (an Hz source would have to
+  // reach the halo recomputation); PFB200_BATCH_SPLIT=1 keeps the split
+  // passes
+  bool any_h = false;
+  for (size_t q = 0; q < b->s_comp.size(); ++q) any_h = any_h || b->s_comp[q] == 2;
+  b->fused = !any_h && !getenv("PFB200_BATCH_SPLIT");
+  if (b->fused) {
+    for (int q = 0; q < 3; ++q)
+      if ((rc = balloc(b, &b->lvl1[q], b->ncell * S))) return rc;
+    for (int q = 0; q < 2; ++q)
+      if ((rc = balloc(b, &b->lvl1[3 + q], b->npsi[q] * S))) return rc;
+  }
   if (!b->fwd_only) {
     for (int q = 0; q < 3; ++q)
       if ((rc = balloc(b, &b->aE[q], b->ncell * S))) return rc;
     for (int q = 0; q < 4; ++q) {
       if ((rc = balloc(b, &b->apsi[q], b->npsi[q] * S))) return rc;
-      if ((rc = balloc(b, &b->g[q], b->ncell * S))) return rc;
+      // hA / hB (g[2], g[3]) live in shared memory on the fused path
+      const bool need = q < 2 || !b->fused;
+      if ((rc = balloc(b, &b->g[q], need ? b->ncell * S : 16))) return rc;
+    }
+    if (b->fused) {
+      const long long n1[5] = {b->ncell, b->npsi[0], b->npsi[1], b->ncell, b->ncell};
+      for (int q = 0; q < 5; ++q)
+        if ((rc = balloc(b, &b->alvl1[q], n1[q] * S))) return rc;
     }
     if ((rc = balloc(b, (void**)&b->grad, b->n_design * 8))) return rc;
     if ((rc = balloc(b, (void**)&b->cot, (size_t)b->nline * b->n_freq * 16))) return rc;
@@ -839,7 +926,9 @@ int pfb_read_field(pf_batch* b, int k, int comp, void* dst) {
   if (!b->finalized || k < 0 || k >= b->n_inst || comp < 0 || comp > 2 || !dst)
     return bfail(b, PF_ERR_INVALID, "bad pfb_read_field");
   const Inst& I = b->inst[k];
-  void* src = comp == 0 ? b->Ex : (comp == 1 ? b->Ey : b->Hz);
+  const bool l1 = level_at(b, b->field_step) == 1;
+  void* src = comp == 0 ? (l1 ? b->lvl1[0] : b->Ex)
+                        : (comp == 1 ? (l1 ? b->lvl1[1] : b->Ey) : (l1 ? b->lvl1[2] : b->Hz));
   B_CUDA(b, cudaMemcpy2DAsync(dst, (size_t)I.ny * b->rb, (char*)src + I.off * b->rb,
                               (size_t)I.pitch * b->rb, (size_t)I.ny * b->rb, I.nx,
                               cudaMemcpyDeviceToHost, b->stream));
@@ -849,15 +938,16 @@ int pfb_read_field(pf_batch* b, int k, int comp, void* dst) {
 
 int pfb_info(const pf_batch* b, int64_t* out, int n_out) {
   if (!b || !out) return PF_ERR_INVALID;
-  const int64_t v[8] = {b->ncell_real,
+  const int64_t v[9] = {b->ncell_real,
                         b->nline,
                         b->n_design,
                         b->ntiles,
                         (int64_t)b->ckpt,
                         (int64_t)((b->n_steps + b->ckpt - 1) / b->ckpt),
                         b->state_elems,
-                        b->launches};
-  for (int q = 0; q < n_out && q < 8; ++q) out[q] = v[q];
+                        b->launches,
+                        b->fused ? 1 : 0};
+  for (int q = 0; q < n_out && q < 9; ++q) out[q] = v[q];
   return PF_OK;
 }
 

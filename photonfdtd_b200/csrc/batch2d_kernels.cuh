@@ -63,6 +63,9 @@ struct BArgs {
   T* ring;                // design-window curls, slot = n mod ring_len
   long long n_design;
   int ring_len;
+  // The fused step's double-buffered state: step n reads level n & 1 and
+  // writes level (n & 1) ^ 1 (level 0 is Ex / Ey / Hz / pHzx / pHzy above).
+  T *Ex2[2], *Ey2[2], *Hz2[2], *pHzx2[2], *pHzy2[2];
 };
 
 // ---- forward ---------------------------------------------------------------
@@ -194,6 +197,203 @@ __global__ void __launch_bounds__(32 * kWarps) kb_e(const __grid_constant__ BArg
   }
 }
 
+// ---- fused forward step ------------------------------------------------------
+// One launch per step on double-buffered fields: a tile first updates Hz of
+// its own cells and, recomputed from the previous level, of the one-cell halo
+// its E update needs (the row above, the column to the left), keeping them in
+// shared memory; then it updates Ex and Ey of its own cells from there.
+// Everything is read from level n & 1 and written to level (n & 1) ^ 1 (the
+// E psi, which no other tile reads, in place), so tiles never race and the
+// fields cross HBM once per step: Ex, Ey, Hz and ce read, Ex, Ey, Hz written.
+// The arithmetic of every cell is kb_h's and kb_e's, operation for operation,
+// so the results equal the split passes' bit for bit. Used when no source
+// drives Hz (an H source would have to reach the halo recomputation).
+
+// Hz^{n+1/2} of cell (i, j) from its own old value and its E neighbours, as
+// kb_h computes it. crow / ccol: pooled x / y coefficient index of the cell;
+// psi_out == nullptr recomputes a halo cell without storing its psi.
+template <typename T>
+__device__ __forceinline__ T hz_value(const BArgs<T>& a, const Inst& I, int i, int j, int ny,
+                                      int crow, int ccol, int mx, int my, T hz, T eyp, T ey,
+                                      T exp_, T ex, const T* pzx, T* pzxo, const T* pzy,
+                                      T* pzyo) {
+  const T mch = -a.ch;
+  const T dA = qdiv(sub_rn(eyp, ey), a.dx, a.rdx, a.fdx);
+  const T dB = qdiv(sub_rn(exp_, ex), a.dy, a.rdy, a.fdy);
+  T h = add_rn(hz, mul_rn(sub_rn(dA, dB), mch));
+  if (mx >= 0) {
+    const long long q = I.p_hzx + (long long)mx * ny + j;
+    const T psi = add_rn(mul_rn(a.bhx[crow], pzx[q]), mul_rn(a.chx[crow], dA));
+    if (pzxo) pzxo[q] = psi;
+    h = add_rn(h, mul_rn(mch, psi));
+  }
+  if (my >= 0) {
+    const long long q = I.p_hzy + (long long)i * I.nphy + my;
+    const T psi = add_rn(mul_rn(a.bhy[ccol], pzy[q]), mul_rn(a.chy[ccol], dB));
+    if (pzyo) pzyo[q] = psi;
+    h = add_rn(h, mul_rn(a.ch, psi));
+  }
+  return h;
+}
+
+template <typename T, int R>
+__global__ void __launch_bounds__(32 * kWarps) kb_step(const __grid_constant__ BArgs<T> a,
+                                                      int step_t) {
+  constexpr int TR = kWarps * R;
+  __shared__ T sH[TR + 1][33];  // [1 + row][1 + column]; row / column 0 = halo
+  const long long n = *a.base + step_t;
+  const int L = (int)(n & 1);
+  const T* Ex = a.Ex2[L];
+  const T* Ey = a.Ey2[L];
+  const T* Hz = a.Hz2[L];
+  T* Exo = a.Ex2[L ^ 1];
+  T* Eyo = a.Ey2[L ^ 1];
+  T* Hzo = a.Hz2[L ^ 1];
+  const T* pzx = a.pHzx2[L];
+  const T* pzy = a.pHzy2[L];
+  T* pzxo = a.pHzx2[L ^ 1];
+  T* pzyo = a.pHzy2[L ^ 1];
+  const int lane = threadIdx.x;
+  const int r0 = threadIdx.y * R;
+  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    const TileRec tr = a.tiles[t];
+    const Inst& I = a.inst[tr.k];
+    const int i = tr.i0 + r0, j = tr.j0 + lane;
+    const bool jv = j < tr.ny;
+    const long long id0 = tr.base + (long long)r0 * tr.pitch + lane;
+    // ---- Hz of the tile's own cells
+    {
+      T ey[R + 1], ex0[R], ex1[R], hz[R];
+      int mx[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const bool ok = jv && i + r < tr.nx;
+        const long long id = id0 + (long long)r * tr.pitch;
+        ey[r] = ok ? Ey[id] : T(0);
+        ex0[r] = ok ? Ex[id] : T(0);
+        ex1[r] = (ok && j + 1 < tr.ny) ? Ex[id + 1] : T(0);
+        hz[r] = ok ? Hz[id] : T(0);
+        mx[r] = ok ? a.mhx[tr.ox + r0 + r] : -1;
+      }
+      ey[R] = (jv && i + R < tr.nx) ? Ey[id0 + (long long)R * tr.pitch] : T(0);
+      const int my = jv ? a.mhy[tr.oy + lane] : -1;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        T h = hz[r];
+        if (jv && i + r < tr.nx - 1 && j < tr.ny - 1)
+          h = hz_value<T>(a, I, i + r, j, tr.ny, tr.ox + r0 + r, tr.oy + lane, mx[r], my, hz[r],
+                          ey[r + 1], ey[r], ex1[r], ex0[r], pzx, pzxo, pzy, pzyo);
+        if (jv && i + r < tr.nx) Hzo[id0 + (long long)r * tr.pitch] = h;
+        sH[r0 + r + 1][lane + 1] = h;
+      }
+    }
+    // ---- halo row i0 - 1 (warp 0), recomputed from level L
+    if (threadIdx.y == 0) {
+      T h = T(0);
+      if (tr.i0 >= 1 && jv) {
+        const long long id = tr.base - tr.pitch + lane;
+        h = Hz[id];
+        if (j < tr.ny - 1) {
+          const int mx = a.mhx[tr.ox - 1];
+          const int my = a.mhy[tr.oy + lane];
+          h = hz_value<T>(a, I, tr.i0 - 1, j, tr.ny, tr.ox - 1, tr.oy + lane, mx, my, h,
+                          Ey[id + tr.pitch], Ey[id], Ex[id + 1], Ex[id], pzx, nullptr, pzy,
+                          nullptr);
+        }
+      }
+      sH[0][lane + 1] = h;
+    }
+    // ---- halo column j0 - 1 (lanes 0 .. R-1 of each warp, one row each)
+    if (lane < R) {
+      const int ih = i + lane;
+      T h = T(0);
+      if (tr.j0 >= 1 && ih < tr.nx) {
+        const long long id = tr.base + (long long)(r0 + lane) * tr.pitch - 1;
+        h = Hz[id];
+        if (ih < tr.nx - 1) {
+          const int mx = a.mhx[tr.ox + r0 + lane];
+          const int my = a.mhy[tr.oy - 1];
+          h = hz_value<T>(a, I, ih, tr.j0 - 1, tr.ny, tr.ox + r0 + lane, tr.oy - 1, mx, my, h,
+                          Ey[id + tr.pitch], Ey[id], Ex[id + 1], Ex[id], pzx, nullptr, pzy,
+                          nullptr);
+        }
+      }
+      sH[r0 + lane + 1][0] = h;
+    }
+    __syncthreads();
+    // ---- Ex, Ey of the tile's own cells (kb_e with Hz from shared memory)
+    {
+      T ex[R], ey[R], K[R];
+      int mx[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const bool ok = jv && i + r < tr.nx;
+        const long long id = id0 + (long long)r * tr.pitch;
+        ex[r] = ok ? Ex[id] : T(0);
+        ey[r] = ok ? Ey[id] : T(0);
+        K[r] = ok ? a.ce[id] : T(0);
+        mx[r] = ok ? a.mex[tr.ox + r0 + r] : -1;
+      }
+      const int my = jv ? a.mey[tr.oy + lane] : -1;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        if (!(jv && i + r < tr.nx)) break;
+        const long long id = id0 + (long long)r * tr.pitch;
+        const T hc = sH[r0 + r + 1][lane + 1];
+        T cx = T(0), cy = T(0);
+        T e = ex[r];
+        if (j >= 1) {
+          const T dA = qdiv(sub_rn(hc, sH[r0 + r + 1][lane]), a.dy, a.rdy, a.fdy);
+          e = add_rn(ex[r], mul_rn(dA, K[r]));
+          cx = dA;
+          if (my >= 0) {
+            const long long q = I.p_exy + (long long)(i + r) * I.npey + my;
+            const int c = tr.oy + lane;
+            const T psi = add_rn(mul_rn(a.bey[c], a.pExy[q]), mul_rn(a.cey[c], dA));
+            a.pExy[q] = psi;
+            e = add_rn(e, mul_rn(K[r], psi));
+            cx = add_rn(dA, psi);
+          }
+        }
+        Exo[id] = e;
+        e = ey[r];
+        if (i + r >= 1) {
+          const T dB = qdiv(sub_rn(hc, sH[r0 + r][lane + 1]), a.dx, a.rdx, a.fdx);
+          e = add_rn(ey[r], mul_rn(-dB, K[r]));
+          cy = -dB;
+          if (mx[r] >= 0) {
+            const long long q = I.p_eyx + (long long)mx[r] * tr.ny + j;
+            const int c = tr.ox + r0 + r;
+            const T psi = add_rn(mul_rn(a.bex[c], a.pEyx[q]), mul_rn(a.cex[c], dB));
+            a.pEyx[q] = psi;
+            e = add_rn(e, mul_rn(-K[r], psi));
+            cy = sub_rn(cy, psi);
+          }
+        }
+        Eyo[id] = e;
+        const int di = r0 + r - tr.wdi, dj = lane - tr.wdj;
+        if (di >= 0 && di < tr.wdn && dj >= 0 && dj < tr.wdn) {
+          const long long slot = n % a.ring_len;
+          T* rr = a.ring + (slot * a.n_design + I.goff + (long long)di * tr.wdn + dj) * 2;
+          rr[0] = cx;
+          rr[1] = cy;
+        }
+      }
+    }
+    __syncthreads();  // sH is rewritten by the next tile
+  }
+}
+
+// Field pointers kb_post writes through: level 0 for the in-place split
+// passes; for the fused step (flip = 1) the level step n has just written.
+template <typename T>
+struct BFields {
+  T* Ex[2];
+  T* Ey[2];
+  T* Hz[2];
+  int flip;
+};
+
 struct BSources {
   const long long* cell;  // pooled cell of each group
   const int* comp;        // 0 Ex, 1 Ey, 2 Hz
@@ -212,14 +412,18 @@ struct BSources {
 // nline threads sample: one launch is correct only when no group of this
 // family sits on a line cell, which the host checks.
 template <typename T>
-__global__ void kb_post(BSources s, T* Ex, T* Ey, T* Hz, int family_h, const long long* base,
+__global__ void kb_post(BSources s, BFields<T> f, int family_h, const long long* base,
                         int step_t, const long long* lcell, long long nline, T* dring) {
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = *base + step_t;
+  const int lv = f.flip ? (int)((n & 1) ^ 1) : 0;
+  T* Ex = f.Ex[lv];
+  T* Ey = f.Ey[lv];
+  T* Hz = f.Hz[lv];
   if (g < s.n_groups) {
     const int c = s.comp[g];
     if ((c == 2) != (family_h != 0)) return;
     T* F = c == 0 ? Ex : (c == 1 ? Ey : Hz);
-    const long long n = *base + step_t;
     T v = F[s.cell[g]];
     for (int q = s.start[g]; q < s.start[g + 1]; ++q)
       v = add_double<T>(v, __dmul_rn(s.amp[q], s.wave[(long long)s.wave_row[q] * s.n_steps + n]));
@@ -279,6 +483,11 @@ struct AArgs {
   const double* phase;                              // exp(i w (n+1) dt), (n_steps, n_freq)
   int n_freq;
   double dt;
+  // The fused reverse step's double-buffered state (level 0 = the arrays
+  // above): the E transpose of step m writes gA / gB into level m & 1; the H
+  // transpose of step n reads aHz and its psi adjoints from level (n + 1) & 1
+  // and writes them into level n & 1.
+  T *aHz2[2], *aHzx2[2], *aHzy2[2], *gA2[2], *gB2[2];
 };
 
 // The adjoint arithmetic is written with explicitly rounded operations, so
@@ -436,6 +645,206 @@ __global__ void __launch_bounds__(32 * kWarps) kb_adj_cell(const __grid_constant
       d.aEx[id] = x;
       d.aEy[id] = y;
     }
+  }
+}
+
+// ---- fused reverse step -------------------------------------------------------
+// One launch per reverse step n, on double-buffered adjoint state: the H
+// transpose of step n (HT: gather gA / gB into aHz, H psi adjoints, hA / hB),
+// the gather of hA / hB into step n's E adjoints, then the E transpose of step
+// n - 1 (ET: line source, design gradient, E psi adjoints, new gA / gB). hA
+// and hB never leave shared memory: a tile recomputes them on its one-cell
+// halo (the row above, the column to the left) from the previous level.
+// Without HT the launch is the E transpose of step n alone (a chunk's first
+// launch); without ET it ends after the gather (its last). Every cell's
+// arithmetic is kb_adj_h's and kb_adj_cell's, operation for operation.
+
+// aHz after the H transpose of one cell and its hA / hB (psi adjoints stored
+// only when the output pointers are given).
+template <typename T>
+__device__ __forceinline__ void adj_h_value(const BArgs<T>& a, const Inst& I, int i, int j,
+                                            int nx, int ny, int crow, int ccol, int mx, int my,
+                                            T ah, T ga0, T ga1, T gb0, T gb1, const T* pzx,
+                                            T* pzxo, const T* pzy, T* pzyo, T& h, T& ha,
+                                            T& hb) {
+  h = fma_rn(sub_rn(gb0, gb1), a.idx, fma_rn(sub_rn(ga0, ga1), a.idy, ah));
+  ha = T(0);
+  hb = T(0);
+  if (i < nx - 1 && j < ny - 1) {
+    ha = mul_rn(-a.ch, h);
+    hb = mul_rn(a.ch, h);
+    if (mx >= 0) {
+      const long long q = I.p_hzx + (long long)mx * ny + j;
+      const T ap = fma_rn(-a.ch, h, pzx[q]);
+      ha = fma_rn(a.chx[crow], ap, ha);
+      if (pzxo) pzxo[q] = mul_rn(a.bhx[crow], ap);
+    }
+    if (my >= 0) {
+      const long long q = I.p_hzy + (long long)i * I.nphy + my;
+      const T ap = fma_rn(a.ch, h, pzy[q]);
+      hb = fma_rn(a.chy[ccol], ap, hb);
+      if (pzyo) pzyo[q] = mul_rn(a.bhy[ccol], ap);
+    }
+  }
+}
+
+template <typename T, int R, bool HT, bool ET>
+__global__ void __launch_bounds__(32 * kWarps) kb_adj_step(const __grid_constant__ BArgs<T> a,
+                                                          const __grid_constant__ AArgs<T> d,
+                                                          int step_t) {
+  constexpr int TR = kWarps * R;
+  __shared__ T sA[TR + 1][33];  // hA: [1 + row][1 + column]; row 0 = halo row
+  __shared__ T sB[TR + 1][33];  // hB: column 0 = halo column
+  const long long n = *a.base + step_t;
+  const long long m = HT ? n - 1 : n;  // the step of the E transpose
+  const int lg = (int)(n & 1);         // gA / gB level the H transpose reads
+  const int lh = (int)((n + 1) & 1);   // aHz / H psi adjoint level it reads
+  const T* gA = d.gA2[lg];
+  const T* gB = d.gB2[lg];
+  T* gAo = d.gA2[(int)(m & 1)];
+  T* gBo = d.gB2[(int)(m & 1)];
+  const T* aHz = d.aHz2[lh];
+  T* aHzo = d.aHz2[lh ^ 1];
+  const T* pzx = d.aHzx2[lh];
+  const T* pzy = d.aHzy2[lh];
+  T* pzxo = d.aHzx2[lh ^ 1];
+  T* pzyo = d.aHzy2[lh ^ 1];
+  const int lane = threadIdx.x;
+  const int r0 = threadIdx.y * R;
+  for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    const TileRec tr = a.tiles[t];
+    const Inst& I = a.inst[tr.k];
+    const int i = tr.i0 + r0, j = tr.j0 + lane;
+    const bool jv = j < tr.ny;
+    const long long id0 = tr.base + (long long)r0 * tr.pitch + lane;
+    if (HT) {
+      // ---- H transpose of the tile's own cells
+      T ah[R], ga0[R], ga1[R], gb[R + 1];
+      int mx[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const bool ok = jv && i + r < tr.nx;
+        const long long id = id0 + (long long)r * tr.pitch;
+        ah[r] = ok ? aHz[id] : T(0);
+        ga0[r] = ok ? gA[id] : T(0);
+        ga1[r] = (ok && j + 1 < tr.ny) ? gA[id + 1] : T(0);
+        gb[r] = ok ? gB[id] : T(0);
+        mx[r] = ok ? a.mhx[tr.ox + r0 + r] : -1;
+      }
+      gb[R] = (jv && i + R < tr.nx) ? gB[id0 + (long long)R * tr.pitch] : T(0);
+      const int my = jv ? a.mhy[tr.oy + lane] : -1;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        T h = T(0), ha = T(0), hb = T(0);
+        if (jv && i + r < tr.nx) {
+          adj_h_value<T>(a, I, i + r, j, tr.nx, tr.ny, tr.ox + r0 + r, tr.oy + lane, mx[r], my,
+                         ah[r], ga0[r], ga1[r], gb[r], gb[r + 1], pzx, pzxo, pzy, pzyo, h, ha,
+                         hb);
+          aHzo[id0 + (long long)r * tr.pitch] = h;
+        }
+        sA[r0 + r + 1][lane + 1] = ha;
+        sB[r0 + r + 1][lane + 1] = hb;
+      }
+      // ---- halo row i0 - 1 (warp 0): its hA, recomputed from the read level
+      if (threadIdx.y == 0) {
+        T ha = T(0);
+        if (tr.i0 >= 1 && jv) {
+          const long long id = tr.base - tr.pitch + lane;
+          T h, hb;
+          adj_h_value<T>(a, I, tr.i0 - 1, j, tr.nx, tr.ny, tr.ox - 1, tr.oy + lane,
+                         a.mhx[tr.ox - 1], a.mhy[tr.oy + lane], aHz[id], gA[id],
+                         j + 1 < tr.ny ? gA[id + 1] : T(0), gB[id], gB[id + tr.pitch], pzx,
+                         nullptr, pzy, nullptr, h, ha, hb);
+        }
+        sA[0][lane + 1] = ha;
+      }
+      // ---- halo column j0 - 1 (lanes 0 .. R-1 of each warp): its hB
+      if (lane < R) {
+        const int ih = i + lane;
+        T hb = T(0);
+        if (tr.j0 >= 1 && ih < tr.nx) {
+          const long long id = tr.base + (long long)(r0 + lane) * tr.pitch - 1;
+          T h, ha;
+          adj_h_value<T>(a, I, ih, tr.j0 - 1, tr.nx, tr.ny, tr.ox + r0 + lane, tr.oy - 1,
+                         a.mhx[tr.ox + r0 + lane], a.mhy[tr.oy - 1], aHz[id], gA[id],
+                         gA[id + 1], gB[id], ih + 1 < tr.nx ? gB[id + tr.pitch] : T(0), pzx,
+                         nullptr, pzy, nullptr, h, ha, hb);
+        }
+        sB[r0 + lane + 1][0] = hb;
+      }
+      __syncthreads();
+    }
+    // ---- E adjoints: finish step n's (HT), then the E transpose of step m (ET)
+    {
+      T lx[R], ly[R], K[R];
+      int mx[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const bool ok = jv && i + r < tr.nx;
+        const long long id = id0 + (long long)r * tr.pitch;
+        lx[r] = ok ? d.aEx[id] : T(0);
+        ly[r] = ok ? d.aEy[id] : T(0);
+        if (ET) {
+          K[r] = ok ? a.ce[id] : T(0);
+          mx[r] = ok ? a.mex[tr.ox + r0 + r] : -1;
+        }
+      }
+      const int my = (ET && jv) ? a.mey[tr.oy + lane] : -1;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        if (!(jv && i + r < tr.nx)) break;
+        const long long id = id0 + (long long)r * tr.pitch;
+        T x = lx[r], y = ly[r];
+        if (HT) {
+          y = fma_rn(sub_rn(sA[r0 + r][lane + 1], sA[r0 + r + 1][lane + 1]), a.idx, y);
+          x = fma_rn(sub_rn(sB[r0 + r + 1][lane], sB[r0 + r + 1][lane + 1]), a.idy, x);
+        }
+        if (ET) {
+          if (i + r == I.line_i) {
+            const double* ph = d.phase + m * d.n_freq * 2;
+            const double* g = d.cot + (I.loff + j) * d.n_freq * 2;
+            double sum = 0.0;
+            for (int f = 0; f < d.n_freq; ++f)
+              sum = __dadd_rn(sum, __dadd_rn(__dmul_rn(g[2 * f], ph[2 * f]),
+                                             __dmul_rn(g[2 * f + 1], ph[2 * f + 1])));
+            y = (T)__dadd_rn((double)y, __dmul_rn(d.dt, sum));
+          }
+          const int di = r0 + r - tr.wdi, dj = lane - tr.wdj;
+          if (di >= 0 && di < tr.wdn && dj >= 0 && dj < tr.wdn) {
+            const long long dc = I.goff + (long long)di * tr.wdn + dj;
+            const T* rr = a.ring + ((m % a.ring_len) * a.n_design + dc) * 2;
+            d.grad[dc] = __dadd_rn(d.grad[dc], __dadd_rn(__dmul_rn((double)x, (double)rr[0]),
+                                                         __dmul_rn((double)y, (double)rr[1])));
+          }
+          T ga = T(0), gbv = T(0);
+          if (j >= 1) {
+            ga = mul_rn(K[r], x);
+            if (my >= 0) {
+              const long long q = I.p_exy + (long long)(i + r) * I.npey + my;
+              const int c = tr.oy + lane;
+              const T ap = fma_rn(K[r], x, d.aExy[q]);
+              ga = fma_rn(a.cey[c], ap, ga);
+              d.aExy[q] = mul_rn(a.bey[c], ap);
+            }
+          }
+          if (i + r >= 1) {
+            gbv = mul_rn(-K[r], y);
+            if (mx[r] >= 0) {
+              const long long q = I.p_eyx + (long long)mx[r] * tr.ny + j;
+              const int c = tr.ox + r0 + r;
+              const T ap = fma_rn(-K[r], y, d.aEyx[q]);
+              gbv = fma_rn(a.cex[c], ap, gbv);
+              d.aEyx[q] = mul_rn(a.bex[c], ap);
+            }
+          }
+          gAo[id] = ga;
+          gBo[id] = gbv;
+        }
+        d.aEx[id] = x;
+        d.aEy[id] = y;
+      }
+    }
+    if (HT) __syncthreads();  // sA / sB are rewritten by the next tile
   }
 }
 

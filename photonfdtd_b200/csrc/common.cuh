@@ -127,6 +127,7 @@ struct StepArgs {
   T* P;
   long long plev;  // reals per polarisation level
   int lvl;         // polarisation level holding P^n (n & 1)
+  int wait_test;   // test hook of the TMA-staged step (pf_set_wait_test)
 };
 
 enum CeMode { kCeCell1 = 0, kCeCell3 = 1, kCeTable = 2 };

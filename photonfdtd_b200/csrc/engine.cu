@@ -121,12 +121,16 @@ struct pf_engine {
   void* media = nullptr;
   double* wave = nullptr;
   int* flag = nullptr;
+  void* region = nullptr;     // pf_read_region staging buffer (grown on demand)
+  size_t region_bytes = 0;
   bool fused = false;
   double rdl[3] = {1, 1, 1};     // RN(1/d) in the real type, per axis
   bool fdiv[3] = {false, false, false};  // reciprocal division verified
   bool tma = false;      // fused path stages planes with TMA
   TmaMaps maps;
   int* tma_err = nullptr;
+  int wait_test = 0;     // pf_set_wait_test: one TMA stage wait runs out
+  long long check_every = 0;  // pf_set_check_every: non-finite scan period
   int fused_ty = 8;      // fused tile height (8 or 16), env PFB200_FUSED_TY
   int fused_chunks = 0;  // x chunks per column (0 = auto), env PFB200_XCHUNKS
 
@@ -494,7 +498,25 @@ StepArgs<T> step_args(pf_engine* e) {
   a.P = (T*)e->P;
   a.plev = e->plev;
   a.lvl = (int)(e->step & 1);
+  a.wait_test = e->wait_test;
   return a;
+}
+
+// Scans the six current fields for inf / nan (synchronous).
+int scan_finite(pf_engine* e) {
+  int* flag = e->flag;
+  PF_CUDA(e, cudaMemsetAsync(flag, 0, sizeof(int), e->stream));
+  for (int c = 0; c < 6; ++c) {
+    const void* f = c < 3 ? e->E[e->cur][c] : e->H[e->cur][c - 3];
+    if (e->rb == 4)
+      k_nonfinite<float><<<592, 256, 0, e->stream>>>((const float*)f, e->ncell, flag);
+    else
+      k_nonfinite<double><<<592, 256, 0, e->stream>>>((const double*)f, e->ncell, flag);
+  }
+  int h = 0;
+  PF_CUDA(e, cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  return h ? fail(e, PF_ERR_NONFINITE, "non-finite field value at step %lld", e->step) : PF_OK;
 }
 
 template <typename T>
@@ -656,6 +678,13 @@ int advance_typed(pf_engine* e, long long n_sub) {
     if (rc) return rc;
     e->cur = nxt;
     e->step++;
+    if (e->check_every > 0 && e->step % e->check_every == 0) {
+      PF_CUDA(e, cudaGetLastError());
+      if ((rc = scan_finite(e))) {
+        collect_profile(e);
+        return rc;
+      }
+    }
   }
   PF_CUDA(e, cudaGetLastError());
   PF_CUDA(e, cudaStreamSynchronize(e->stream));
@@ -1007,6 +1036,57 @@ int pf_read_flux(pf_engine* e, int mon, double* dst) {
   return PF_OK;
 }
 
+int pf_read_region(pf_engine* e, int comp, const int32_t start[3], const int32_t stop[3],
+                   const int32_t stride[3], void* dst) {
+  if (!e || !dst || !start || !stop || !stride) return PF_ERR_INVALID;
+  if (!e->finalized) return fail(e, PF_ERR_STATE, "pf_read_region before pf_finalize");
+  if (!valid_comp(comp)) return fail(e, PF_ERR_INVALID, "bad component %d", comp);
+  const int dims[3] = {e->nx, e->ny, e->nz};
+  int cnt[3];
+  for (int a = 0; a < 3; ++a) {
+    if (stride[a] < 1 || start[a] < 0 || stop[a] > dims[a] || start[a] >= stop[a])
+      return fail(e, PF_ERR_INVALID, "bad region on axis %d", a);
+    cnt[a] = (stop[a] - start[a] + stride[a] - 1) / stride[a];
+  }
+  const long long n = (long long)cnt[0] * cnt[1] * cnt[2];
+  const size_t bytes = (size_t)n * e->rb;
+  PF_CUDA(e, cudaSetDevice(e->device));
+  const void* src = comp < 3 ? e->E[e->cur][comp] : e->H[e->cur][comp - 3];
+  if (n == e->ncell) {  // the whole field: no gather
+    PF_CUDA(e, cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, e->stream));
+    PF_CUDA(e, cudaStreamSynchronize(e->stream));
+    return PF_OK;
+  }
+  if (bytes > e->region_bytes) {
+    if (e->region) {
+      PF_CUDA(e, cudaStreamSynchronize(e->stream));
+      cudaFree(e->region);
+      e->dev_bytes -= e->region_bytes;
+      e->region = nullptr;
+      e->region_bytes = 0;
+    }
+    const cudaError_t rc = cudaMalloc(&e->region, bytes);
+    if (rc != cudaSuccess)
+      return fail(e, PF_ERR_OOM, "CUDA error: cudaMalloc of %zu bytes failed", bytes);
+    e->region_bytes = bytes;
+    e->dev_bytes += bytes;
+  }
+  const int3 st = make_int3(start[0], start[1], start[2]);
+  const int3 sd = make_int3(stride[0], stride[1], stride[2]);
+  const int3 ct = make_int3(cnt[0], cnt[1], cnt[2]);
+  const unsigned g = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
+  if (e->rb == 4)
+    k_gather_region<float><<<g, 256, 0, e->stream>>>((const float*)src, e->ny, e->nz, st, sd, ct,
+                                                     (float*)e->region);
+  else
+    k_gather_region<double><<<g, 256, 0, e->stream>>>((const double*)src, e->ny, e->nz, st, sd,
+                                                      ct, (double*)e->region);
+  PF_CUDA(e, cudaGetLastError());
+  PF_CUDA(e, cudaMemcpyAsync(dst, e->region, bytes, cudaMemcpyDeviceToHost, e->stream));
+  PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  return PF_OK;
+}
+
 int pf_write_field(pf_engine* e, int comp, const void* src) {
   if (!e || !src) return PF_ERR_INVALID;
   if (!e->finalized) return fail(e, PF_ERR_STATE, "pf_write_field before pf_finalize");
@@ -1102,19 +1182,21 @@ int pf_step(const pf_engine* e, int64_t* step) {
 int pf_check_finite(pf_engine* e) {
   if (!e) return PF_ERR_INVALID;
   if (!e->finalized) return fail(e, PF_ERR_STATE, "pf_check_finite before pf_finalize");
-  int* flag = e->flag;
-  PF_CUDA(e, cudaMemsetAsync(flag, 0, sizeof(int), e->stream));
-  for (int c = 0; c < 6; ++c) {
-    const void* f = c < 3 ? e->E[e->cur][c] : e->H[e->cur][c - 3];
-    if (e->rb == 4)
-      k_nonfinite<float><<<592, 256, 0, e->stream>>>((const float*)f, e->ncell, flag);
-    else
-      k_nonfinite<double><<<592, 256, 0, e->stream>>>((const double*)f, e->ncell, flag);
-  }
-  int h = 0;
-  PF_CUDA(e, cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
-  PF_CUDA(e, cudaStreamSynchronize(e->stream));
-  return h ? fail(e, PF_ERR_NONFINITE, "non-finite field value at step %lld", e->step) : PF_OK;
+  PF_CUDA(e, cudaSetDevice(e->device));
+  return scan_finite(e);
+}
+
+int pf_set_check_every(pf_engine* e, int64_t k) {
+  if (!e) return PF_ERR_INVALID;
+  if (k < 0) return fail(e, PF_ERR_INVALID, "check period must be >= 0");
+  e->check_every = k;
+  return PF_OK;
+}
+
+int pf_set_wait_test(pf_engine* e, int on) {
+  if (!e) return PF_ERR_INVALID;
+  e->wait_test = on ? 1 : 0;
+  return PF_OK;
 }
 
 int pf_stream(const pf_engine* e, void** stream) {
@@ -1167,6 +1249,7 @@ void pf_destroy(pf_engine* e) {
   if (!e) return;
   if (e->stream) cudaStreamSynchronize(e->stream);
   for (void* p : e->allocs) cudaFree(p);
+  if (e->region) cudaFree(e->region);
   for (cudaEvent_t ev : e->ev_pool) cudaEventDestroy(ev);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;

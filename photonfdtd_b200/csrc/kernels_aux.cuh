@@ -204,6 +204,21 @@ __global__ void __launch_bounds__(256) k_flux_flush(const double* partial, int n
   if (threadIdx.x == 0) *acc = total;
 }
 
+// Strided sub-block of one field into a compact C-order buffer (the
+// FieldMonitor snapshot: every stride-th cell per axis, or one z plane).
+template <typename T>
+__global__ void k_gather_region(const T* f, int ny, int nz, int3 start, int3 stride,
+                                int3 count, T* out) {
+  const long long n = (long long)count.x * count.y * count.z;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long ck = t % count.z, rest = t / count.z;
+    const long long cj = rest % count.y, ci = rest / count.y;
+    out[t] = f[((long long)(start.x + ci * stride.x) * ny + (start.y + cj * stride.y)) * nz +
+               (start.z + ck * stride.z)];
+  }
+}
+
 // Non-finite scan over a field: sets *flag when any value is inf or nan.
 template <typename T>
 __global__ void k_nonfinite(const T* f, long long n, int* flag) {

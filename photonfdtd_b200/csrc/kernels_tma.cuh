@@ -57,8 +57,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   return ok != 0;
 }
 // Bounded wait; returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-  for (long long t = 0; t < kWaitLimit; ++t)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity,
+                                          long long limit = kWaitLimit) {
+  for (long long t = 0; t < limit; ++t)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -109,6 +110,9 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY))
   Stage* st = reinterpret_cast<Stage*>(((uintptr_t)dyn + 127) & ~(uintptr_t)127);
   __shared__ T sh[3][TY + 1][TZ + 1];
   __shared__ __align__(8) uint64_t full[NS];
+  // Test hook (a.wait_test): block (0, 0, 0) waits once on this barrier,
+  // which nothing arrives on, with a short limit, and takes the timeout path.
+  __shared__ __align__(8) uint64_t never;
   __shared__ MediumT<T> smed[ADE ? kMaxMedia : 1];
 
   const int tz = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tz;
@@ -152,8 +156,10 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY))
   if (__syncthreads_or(misaligned)) return;
   if (tid == 0) {
     for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
+    mbar_init(&never, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  const bool test_block = a.wait_test && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0;
   if (ADE && tid < a.n_media) smed[tid] = a.media[tid];
   __syncthreads();
   if (tid == 0)
@@ -184,8 +190,13 @@ __global__ void __launch_bounds__(32 * TY, 1024 / (32 * TY))
 
   for (int i = ib; i < ie; ++i) {
     const int q0 = i - ib, q1 = q0 + 1;
-    bool ok = mbar_wait(&full[q0 % NS], (unsigned)((q0 / NS) & 1));
-    ok = ok && mbar_wait(&full[q1 % NS], (unsigned)((q1 / NS) & 1));
+    bool ok;
+    if (test_block && i == ib) {
+      ok = mbar_wait(&never, 0u, 1 << 12);  // runs out: nothing arrives
+    } else {
+      ok = mbar_wait(&full[q0 % NS], (unsigned)((q0 / NS) & 1));
+      ok = ok && mbar_wait(&full[q1 % NS], (unsigned)((q1 / NS) & 1));
+    }
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {
         atomicExch(err, 1);

@@ -212,13 +212,14 @@ __device__ __forceinline__ bool tc_mbar_try(uint32_t bar, uint32_t parity) {
 }
 
 // Waits for the completion of the phase with the given parity, at most
-// kTcWaitNs (and at most 2^30 polls); gives up early once *abort is set.
+// limit_ns (and at most 2^30 polls); gives up early once *abort is set.
 __device__ __forceinline__ bool tc_mbar_wait(uint32_t bar, uint32_t parity,
-                                             const volatile int* abort = nullptr) {
+                                             const volatile int* abort = nullptr,
+                                             unsigned long long limit_ns = kTcWaitNs) {
   const unsigned long long t0 = tc_now();
   for (int i = 0; i < (1 << 30); ++i) {
     if (tc_mbar_try(bar, parity)) return true;
-    if ((i & 63) == 63 && (tc_now() - t0 > kTcWaitNs || (abort && *abort))) return false;
+    if ((i & 63) == 63 && (tc_now() - t0 > limit_ns || (abort && *abort))) return false;
   }
   return false;
 }
@@ -241,11 +242,15 @@ template <int BN>
 __global__ void __launch_bounds__(128, 1)
     k_gemm_tc(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
               int M, int N, int K, float* C, int ldc, float alpha, float beta, int kc, float* work,
-              int* err) {
+              int* err, int wait_test) {
   static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "BN");
   constexpr uint32_t ABYTES = TBM * TBK * 2, SB = tc_stage_bytes(BN);
   extern __shared__ uint8_t tc_smem[];
   __shared__ __align__(8) uint64_t full[TC_STAGES], empty[TC_STAGES], done;
+  // Test hook (pfs_gemm_wait_test): the MMA warp of block (0, 0, 0) first
+  // waits 100 us on this barrier, which nothing arrives on, and so takes the
+  // timeout path below.
+  __shared__ __align__(8) uint64_t never;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag, n_loaded, n_seen;
   volatile int* abort_v = &abort_flag;
@@ -272,6 +277,7 @@ __global__ void __launch_bounds__(128, 1)
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[i])));
     }
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&done)));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&never)));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     abort_flag = 0;
     n_loaded = 0;
@@ -306,9 +312,12 @@ __global__ void __launch_bounds__(128, 1)
     constexpr uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) |
                                ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TBM >> 4) << 24);
     int kt = 0;
+    const bool test_block = wait_test && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0;
     for (; kt < nk; ++kt) {
       const int st = kt % TC_STAGES;
-      const bool ok = tc_mbar_wait(smem_u32(&full[st]), (kt / TC_STAGES) & 1, abort_v);
+      const bool ok = (test_block && kt == 0)
+                          ? tc_mbar_wait(smem_u32(&never), 0, abort_v, 100000ull)
+                          : tc_mbar_wait(smem_u32(&full[st]), (kt / TC_STAGES) & 1, abort_v);
       if (!__all_sync(0xffffffffu, ok && !*abort_v)) {
         if (lane == 0) *abort_v = 1;
         break;
@@ -348,7 +357,7 @@ __global__ void __launch_bounds__(128, 1)
     if (tid == 0) {
       for (int kt = n_seen; kt < n_loaded; ++kt)
         tc_mbar_wait(smem_u32(&full[kt % TC_STAGES]), (kt / TC_STAGES) & 1);
-      atomicExch(err, 1);
+      atomicAdd(err, 1);
     }
   } else {
     asm volatile("tcgen05.fence::after_thread_sync;");
@@ -709,6 +718,7 @@ bool tc_map(CUtensorMap* m, const void* ptr, int cols, int rows, int ld, int box
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 int g_gemm_engine = 1;  // 1: tcgen05 (TMEM accumulator), 0: mma.sync m16n8k16
+int g_gemm_wait_test = 0;  // pfs_gemm_wait_test
 
 // Launches the GEMM (split over `sz` K slices of kc when sz > 1).
 int launch_gemm(int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B,
@@ -751,19 +761,19 @@ int launch_gemm(int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv
   switch (bn) {
     case 32:
       k_gemm_tc<32><<<grid, 128, tc_smem_bytes(32), st>>>(ta, tb, M, N, K, C, ldc, alpha, beta,
-                                                          kc, work, err);
+                                                          kc, work, err, g_gemm_wait_test);
       break;
     case 64:
       k_gemm_tc<64><<<grid, 128, tc_smem_bytes(64), st>>>(ta, tb, M, N, K, C, ldc, alpha, beta,
-                                                          kc, work, err);
+                                                          kc, work, err, g_gemm_wait_test);
       break;
     case 128:
       k_gemm_tc<128><<<grid, 128, tc_smem_bytes(128), st>>>(ta, tb, M, N, K, C, ldc, alpha, beta,
-                                                            kc, work, err);
+                                                            kc, work, err, g_gemm_wait_test);
       break;
     default:
       k_gemm_tc<256><<<grid, 128, tc_smem_bytes(256), st>>>(ta, tb, M, N, K, C, ldc, alpha, beta,
-                                                            kc, work, err);
+                                                            kc, work, err, g_gemm_wait_test);
   }
   return PF_OK;
 }
@@ -785,6 +795,12 @@ const char* pfs_last_error(void) { return g_err.c_str(); }
 int pfs_gemm_engine(int engine) {
   const int old = g_gemm_engine;
   if (engine == 0 || engine == 1) g_gemm_engine = engine;
+  return old;
+}
+
+int pfs_gemm_wait_test(int on) {
+  const int old = g_gemm_wait_test;
+  if (on == 0 || on == 1) g_gemm_wait_test = on;
   return old;
 }
 

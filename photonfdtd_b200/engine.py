@@ -398,6 +398,20 @@ class B200Engine:
             self._cache[comp] = out
         return self._cache[comp]
 
+    def get_region(self, comp: str, start, stop, stride) -> np.ndarray:
+        """f[start:stop:stride] per axis of one current field, gathered on
+        the device (pf_read_region); only the snapshot is copied out."""
+        import ctypes as C
+        st = np.array(start, np.int32)
+        sp = np.array(stop, np.int32)
+        sd = np.array(stride, np.int32)
+        shape = tuple(len(range(a, b, c)) for a, b, c in zip(st, sp, sd))
+        out = np.empty(shape, dtype=self.npdt)
+        self._chk(self._L.pf_read_region(self.h, _COMP[comp], N.ptr(st, C.c_int32),
+                                         N.ptr(sp, C.c_int32), N.ptr(sd, C.c_int32),
+                                         N.ptr(out)))
+        return out
+
     def set_field(self, comp: str, arr: np.ndarray) -> None:
         """Overwrite one component of the current state (pf_write_field)."""
         src = np.ascontiguousarray(arr, dtype=self.npdt)
@@ -477,6 +491,10 @@ class B200Engine:
     def check_finite(self) -> None:
         self._chk(self._L.pf_check_finite(self.h))
 
+    def set_check_every(self, k: int) -> None:
+        """Scan for inf / nan every k steps while advancing (0: off)."""
+        self._chk(self._L.pf_set_check_every(self.h, int(k)))
+
     def close(self) -> None:
         if getattr(self, "h", None) is not None and self.h.value:
             self._L.pf_destroy(self.h)
@@ -516,6 +534,10 @@ def _result_cls(sim):
 def run_b200(sim, kernel: int = N.PF_KERNEL_AUTO):
     """Run ``sim`` on the B200 engine and return a Result.
 
+    With ``sim.b200_check_every = k``, the engine scans the fields every k
+    steps and raises NativeError (PF_ERR_NONFINITE) at the first inf / nan,
+    e.g. a scene stepped past its Courant limit.
+
     With ``sim.b200_error_vs_f64 = True`` on a float32 scene, the Result also
     carries ``error_vs_f64``: every output's error against a float64 run of
     the same scene on the engine (photonfdtd_b200.accuracy), whose float64
@@ -527,6 +549,9 @@ def run_b200(sim, kernel: int = N.PF_KERNEL_AUTO):
     t1 = time.perf_counter()
     eng = B200Engine(t, kernel=kernel)
     t2 = time.perf_counter()
+    check = int(getattr(sim, "b200_check_every", 0) or 0)
+    if check:
+        eng.set_check_every(check)
     try:
         res = drive(sim, eng, t)
     finally:
@@ -590,19 +615,17 @@ def drive(sim, eng: B200Engine, t: dict, mon_dtype=None):
             steps = {int(round(tt / dt)) for tt in m.times if 0 <= int(round(tt / dt)) < n_steps}
         else:
             steps = set(range(0, n_steps, m.interval))
-        zsl = slice(None)
+        # the snapshot region (simulation.py:1062-1067): one z plane with
+        # plane_z, else every downsample-th cell per axis
+        ds = max(int(m.downsample), 1)
+        shape = tuple(grid.shape)
         if m.plane_z is not None:
             zi = _nearest(grid.coords[2], m.plane_z)
-            zsl = slice(zi, zi + 1)
-        rec[m.name] = dict(m=m, steps=steps, zsl=zsl, n=len(steps), count=0,
+            region = ((0, 0, zi), (shape[0], shape[1], zi + 1), (ds, ds, 1))
+        else:
+            region = ((0, 0, 0), shape, (ds, ds, ds))
+        rec[m.name] = dict(m=m, steps=steps, region=region, n=len(steps), count=0,
                            store={c: None for c in m.components}, times=[])
-
-    def snap_view(f, ds, zsl):
-        if zsl != slice(None):
-            return f[::ds, ::ds, zsl]
-        if ds > 1:
-            return f[::ds, ::ds, ::ds]
-        return f
 
     stop_steps = sorted(set().union(*(r["steps"] for r in rec.values()))) if rec else []
     cb = getattr(sim, "progress_callback", None)
@@ -625,7 +648,7 @@ def drive(sim, eng: B200Engine, t: dict, mon_dtype=None):
                 continue
             m = r["m"]
             for c in m.components:
-                snap = snap_view(eng.get(c), m.downsample, r["zsl"])
+                snap = eng.get_region(c, *r["region"])
                 if r["store"][c] is None:
                     r["store"][c] = np.empty((r["n"],) + snap.shape, dtype=mon_dtype)
                 r["store"][c][r["count"]] = snap

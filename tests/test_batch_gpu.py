@@ -190,3 +190,33 @@ def test_adjoint_needs_a_forward_of_the_current_design():
             b.adjoint(g[:-1])
     finally:
         b.close()
+
+
+@pytest.mark.parametrize("precision", ["float32", "float64"])
+def test_fused_steps_equal_split_passes(precision, monkeypatch):
+    """The fused forward step (one launch per step, double-buffered fields,
+    recomputed Hz halo) and the fused reverse step (hA / hB recomputed on the
+    halo in shared memory) against the split passes: line DFT, final fields
+    and the adjoint gradient bit for bit, with an odd checkpoint spacing so
+    that chunks start on both levels."""
+    sims, _, wins = _sims(precision, 200)
+    out = {}
+    for split in (False, True):
+        if split:
+            monkeypatch.setenv("PFB200_BATCH_SPLIT", "1")
+        else:
+            monkeypatch.delenv("PFB200_BATCH_SPLIT", raising=False)
+        b = BatchTE(sims, wins, checkpoint_every=37, tile_rows=(32, 16)[int(split)])
+        try:
+            assert b.info()["fused"] == (0 if split else 1)
+            F = b.forward()
+            fields = [b.read_field(k, c) for k in range(len(sims)) for c in ("Ex", "Ey", "Hz")]
+            g = b.adjoint(objective_cotangent(F))
+            out[split] = (F, fields, g)
+        finally:
+            b.close()
+    (F0, f0, g0), (F1, f1, g1) = out[False], out[True]
+    assert np.array_equal(F0, F1)
+    for a, c in zip(f0, f1):
+        assert np.array_equal(a, c)
+    assert np.array_equal(g0, g1)
