@@ -376,6 +376,25 @@ const char *pfb_last_error(const pf_batch *b);
 void pfb_destroy(pf_batch *b);
 
 /* ------------------------------------------------------------------------
+ * The density chain of topology optimisation (pfd_*), replacing the
+ * reference's JAX conic_filter + tanh_projection (src/photonfdtd/design.py:
+ * 40-72) and the density end of value_and_grad_density (:164-175). A batch of
+ * n_inst windows of n x n raw densities (float64, device pointers, window k
+ * at k * n * n, row-major), n <= 96, filter radius R (cells) <= 32:
+ *   rho_phys = tanh_projection(conic_filter(rho, R), beta, eta), where the
+ *   filter is the normalised same-size convolution with the cone
+ *   max(0, 1 - |d| / R) (R < 1: none) and the projection
+ *   (tanh(beta eta) + tanh(beta (y - eta))) / (tanh(beta eta) +
+ *   tanh(beta (1 - eta))) (beta = 0: none).
+ * pfd_density_backward: grad_rho = (d rho_phys / d rho)^T grad_phys.
+ * Asynchronous on `stream`; allocate nothing. Error text: pfd_last_error(). */
+const char *pfd_last_error(void);
+int pfd_density_forward(int n_inst, int n, const double *rho, double radius, double beta,
+                        double eta, double *rho_phys, void *stream);
+int pfd_density_backward(int n_inst, int n, const double *rho, double radius, double beta,
+                         double eta, const double *grad_phys, double *grad_rho, void *stream);
+
+/* ------------------------------------------------------------------------
  * Surrogate network kernels (pfs_*). The reference has no learned surrogate:
  * these are the training and inference routines of this library's
  * convolutional encoder-decoder (photonfdtd_b200/surrogate.py), which maps

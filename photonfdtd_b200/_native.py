@@ -110,6 +110,10 @@ SIGNATURES = {
     "pfs_gemm_engine": (C.c_int, [C.c_int]),
     "pfs_gemm_timeouts": (C.c_int, [C.POINTER(C.c_int), C.c_int]),
     "pfs_gemm_wait_test": (C.c_int, [C.c_int]),
+    "pfd_last_error": (C.c_char_p, []),
+    "pfd_density_forward": (C.c_int, [C.c_int, C.c_int, _vp, _dbl, _dbl, _dbl, _vp, _vp]),
+    "pfd_density_backward": (C.c_int, [C.c_int, C.c_int, _vp, _dbl, _dbl, _dbl, _vp, _vp,
+                                       _vp]),
     "pfs_im2col": (C.c_int, [C.c_int] * 9 + [_vp, _vp, C.c_int, _vp]),
     "pfs_col2im": (C.c_int, [C.c_int] * 9 + [_vp, C.c_int, _vp, _vp]),
     "pfs_bias_act": (C.c_int, [_i64, C.c_int, _vp, _vp, C.c_int, _vp, _vp, _vp]),
