@@ -571,6 +571,8 @@ def adjoint_bench(iters: int, cpu: bool, n_inst: int = 256, n_steps: int = 4000)
                            "frac": round(adj_bytes / min(adj) / 1e9 / peak, 4),
                            "bytes_per_cell_step": round(adj_bytes / cells, 2)}},
            "checkpoint_every": info["checkpoint_every"], "segments": info["segments"],
+           "fused_steps": bool(info["fused"]), "tile_rows": b.tile_rows,
+           "tile_ms_per_step": b.tile_ms_per_step,
            "setup_s": round(setup, 2), "gpu_launches_per_iter": int(launches),
            "objective_sum": float(np.sum(vals)), "grad_max": float(np.max(np.abs(grad)))}
     b.close()

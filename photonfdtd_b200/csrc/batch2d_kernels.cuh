@@ -21,6 +21,14 @@ namespace pfb {
 namespace b2d {
 
 constexpr int kWarps = 8;     // warps per block
+// Minimum resident blocks per SM the fused forward and reverse steps are
+// compiled for.
+#ifndef PFB_MINB_STEP
+#define PFB_MINB_STEP 4
+#endif
+#ifndef PFB_MINB_ASTEP
+#define PFB_MINB_ASTEP 4
+#endif
 constexpr int kDftRing = 32;  // line samples kept before a DFT flush
 
 struct Inst {
@@ -236,10 +244,16 @@ __device__ __forceinline__ T hz_value(const BArgs<T>& a, const Inst& I, int i, i
   return h;
 }
 
+// Every global load of a tile is issued before its barrier: the own cells'
+// E and H values, coefficients and CPML maps (the E update reuses the Ex / Ey
+// values the H update loaded), the halo row's inputs (warp 0) and the halo
+// column's (warp 1, one row per lane), so a block waits out one memory
+// latency per tile.
 template <typename T, int R>
-__global__ void __launch_bounds__(32 * kWarps) kb_step(const __grid_constant__ BArgs<T> a,
-                                                      int step_t) {
+__global__ void __launch_bounds__(32 * kWarps, PFB_MINB_STEP) kb_step(
+    const __grid_constant__ BArgs<T> a, int step_t) {
   constexpr int TR = kWarps * R;
+  static_assert(TR <= 32, "the halo column is one warp's work");
   __shared__ T sH[TR + 1][33];  // [1 + row][1 + column]; row / column 0 = halo
   const long long n = *a.base + step_t;
   const int L = (int)(n & 1);
@@ -261,123 +275,118 @@ __global__ void __launch_bounds__(32 * kWarps) kb_step(const __grid_constant__ B
     const int i = tr.i0 + r0, j = tr.j0 + lane;
     const bool jv = j < tr.ny;
     const long long id0 = tr.base + (long long)r0 * tr.pitch + lane;
+    // ---- loads: own cells
+    T ey[R + 1], ex0[R], ex1[R], hz[R], K[R];
+    int mxh[R], mxe[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const bool ok = jv && i + r < tr.nx;
+      const long long id = id0 + (long long)r * tr.pitch;
+      ey[r] = ok ? Ey[id] : T(0);
+      ex0[r] = ok ? Ex[id] : T(0);
+      ex1[r] = (ok && j + 1 < tr.ny) ? Ex[id + 1] : T(0);
+      hz[r] = ok ? Hz[id] : T(0);
+      K[r] = ok ? a.ce[id] : T(0);
+      mxh[r] = ok ? a.mhx[tr.ox + r0 + r] : -1;
+      mxe[r] = ok ? a.mex[tr.ox + r0 + r] : -1;
+    }
+    ey[R] = (jv && i + R < tr.nx) ? Ey[id0 + (long long)R * tr.pitch] : T(0);
+    const int myh = jv ? a.mhy[tr.oy + lane] : -1;
+    const int mye = jv ? a.mey[tr.oy + lane] : -1;
+    // ---- loads: the halo cell this thread recomputes, if any (warp 0: row
+    // i0 - 1 at column j; warp 1: column j0 - 1 at tile row `lane`)
+    int hrole = 0;  // 1 halo row, 2 halo column
+    int hi = 0, hj = 0, hcrow = 0, hccol = 0, hmx = -1, hmy = -1;
+    T hz_h = T(0), hey1 = T(0), hey0 = T(0), hex1 = T(0), hex0 = T(0);
+    if (threadIdx.y == 0 && tr.i0 >= 1 && jv) {
+      hrole = 1;
+      hi = tr.i0 - 1;
+      hj = j;
+      hcrow = tr.ox - 1;
+      hccol = tr.oy + lane;
+    } else if (threadIdx.y == 1 && lane < TR && tr.j0 >= 1 && tr.i0 + lane < tr.nx) {
+      hrole = 2;
+      hi = tr.i0 + lane;
+      hj = tr.j0 - 1;
+      hcrow = tr.ox + lane;
+      hccol = tr.oy - 1;
+    }
+    const bool hupd = hrole && hi < tr.nx - 1 && hj < tr.ny - 1;
+    if (hrole) {
+      const long long id = tr.base + (long long)(hi - tr.i0) * tr.pitch + (hj - tr.j0);
+      hz_h = Hz[id];
+      if (hupd) {
+        hey1 = Ey[id + tr.pitch];
+        hey0 = Ey[id];
+        hex1 = Ex[id + 1];
+        hex0 = Ex[id];
+        hmx = a.mhx[hcrow];
+        hmy = a.mhy[hccol];
+      }
+    }
     // ---- Hz of the tile's own cells
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      T h = hz[r];
+      if (jv && i + r < tr.nx - 1 && j < tr.ny - 1)
+        h = hz_value<T>(a, I, i + r, j, tr.ny, tr.ox + r0 + r, tr.oy + lane, mxh[r], myh, hz[r],
+                        ey[r + 1], ey[r], ex1[r], ex0[r], pzx, pzxo, pzy, pzyo);
+      if (jv && i + r < tr.nx) Hzo[id0 + (long long)r * tr.pitch] = h;
+      sH[r0 + r + 1][lane + 1] = h;
+    }
+    // ---- the halo cell, recomputed from level L (its psi is not stored)
     {
-      T ey[R + 1], ex0[R], ex1[R], hz[R];
-      int mx[R];
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const bool ok = jv && i + r < tr.nx;
-        const long long id = id0 + (long long)r * tr.pitch;
-        ey[r] = ok ? Ey[id] : T(0);
-        ex0[r] = ok ? Ex[id] : T(0);
-        ex1[r] = (ok && j + 1 < tr.ny) ? Ex[id + 1] : T(0);
-        hz[r] = ok ? Hz[id] : T(0);
-        mx[r] = ok ? a.mhx[tr.ox + r0 + r] : -1;
-      }
-      ey[R] = (jv && i + R < tr.nx) ? Ey[id0 + (long long)R * tr.pitch] : T(0);
-      const int my = jv ? a.mhy[tr.oy + lane] : -1;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        T h = hz[r];
-        if (jv && i + r < tr.nx - 1 && j < tr.ny - 1)
-          h = hz_value<T>(a, I, i + r, j, tr.ny, tr.ox + r0 + r, tr.oy + lane, mx[r], my, hz[r],
-                          ey[r + 1], ey[r], ex1[r], ex0[r], pzx, pzxo, pzy, pzyo);
-        if (jv && i + r < tr.nx) Hzo[id0 + (long long)r * tr.pitch] = h;
-        sH[r0 + r + 1][lane + 1] = h;
-      }
-    }
-    // ---- halo row i0 - 1 (warp 0), recomputed from level L
-    if (threadIdx.y == 0) {
-      T h = T(0);
-      if (tr.i0 >= 1 && jv) {
-        const long long id = tr.base - tr.pitch + lane;
-        h = Hz[id];
-        if (j < tr.ny - 1) {
-          const int mx = a.mhx[tr.ox - 1];
-          const int my = a.mhy[tr.oy + lane];
-          h = hz_value<T>(a, I, tr.i0 - 1, j, tr.ny, tr.ox - 1, tr.oy + lane, mx, my, h,
-                          Ey[id + tr.pitch], Ey[id], Ex[id + 1], Ex[id], pzx, nullptr, pzy,
-                          nullptr);
-        }
-      }
-      sH[0][lane + 1] = h;
-    }
-    // ---- halo column j0 - 1 (lanes 0 .. R-1 of each warp, one row each)
-    if (lane < R) {
-      const int ih = i + lane;
-      T h = T(0);
-      if (tr.j0 >= 1 && ih < tr.nx) {
-        const long long id = tr.base + (long long)(r0 + lane) * tr.pitch - 1;
-        h = Hz[id];
-        if (ih < tr.nx - 1) {
-          const int mx = a.mhx[tr.ox + r0 + lane];
-          const int my = a.mhy[tr.oy - 1];
-          h = hz_value<T>(a, I, ih, tr.j0 - 1, tr.ny, tr.ox + r0 + lane, tr.oy - 1, mx, my, h,
-                          Ey[id + tr.pitch], Ey[id], Ex[id + 1], Ex[id], pzx, nullptr, pzy,
-                          nullptr);
-        }
-      }
-      sH[r0 + lane + 1][0] = h;
+      T h = hz_h;
+      if (hupd)
+        h = hz_value<T>(a, I, hi, hj, tr.ny, hcrow, hccol, hmx, hmy, hz_h, hey1, hey0, hex1,
+                        hex0, pzx, nullptr, pzy, nullptr);
+      if (threadIdx.y == 0) sH[0][lane + 1] = hrole == 1 ? h : T(0);
+      if (threadIdx.y == 1 && lane < TR) sH[lane + 1][0] = hrole == 2 ? h : T(0);
     }
     __syncthreads();
-    // ---- Ex, Ey of the tile's own cells (kb_e with Hz from shared memory)
-    {
-      T ex[R], ey[R], K[R];
-      int mx[R];
+    // ---- Ex, Ey of the tile's own cells (kb_e's arithmetic, Hz from shared memory)
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const bool ok = jv && i + r < tr.nx;
-        const long long id = id0 + (long long)r * tr.pitch;
-        ex[r] = ok ? Ex[id] : T(0);
-        ey[r] = ok ? Ey[id] : T(0);
-        K[r] = ok ? a.ce[id] : T(0);
-        mx[r] = ok ? a.mex[tr.ox + r0 + r] : -1;
+    for (int r = 0; r < R; ++r) {
+      if (!(jv && i + r < tr.nx)) break;
+      const long long id = id0 + (long long)r * tr.pitch;
+      const T hc = sH[r0 + r + 1][lane + 1];
+      T cx = T(0), cy = T(0);
+      T e = ex0[r];
+      if (j >= 1) {
+        const T dA = qdiv(sub_rn(hc, sH[r0 + r + 1][lane]), a.dy, a.rdy, a.fdy);
+        e = add_rn(ex0[r], mul_rn(dA, K[r]));
+        cx = dA;
+        if (mye >= 0) {
+          const long long q = I.p_exy + (long long)(i + r) * I.npey + mye;
+          const int c = tr.oy + lane;
+          const T psi = add_rn(mul_rn(a.bey[c], a.pExy[q]), mul_rn(a.cey[c], dA));
+          a.pExy[q] = psi;
+          e = add_rn(e, mul_rn(K[r], psi));
+          cx = add_rn(dA, psi);
+        }
       }
-      const int my = jv ? a.mey[tr.oy + lane] : -1;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        if (!(jv && i + r < tr.nx)) break;
-        const long long id = id0 + (long long)r * tr.pitch;
-        const T hc = sH[r0 + r + 1][lane + 1];
-        T cx = T(0), cy = T(0);
-        T e = ex[r];
-        if (j >= 1) {
-          const T dA = qdiv(sub_rn(hc, sH[r0 + r + 1][lane]), a.dy, a.rdy, a.fdy);
-          e = add_rn(ex[r], mul_rn(dA, K[r]));
-          cx = dA;
-          if (my >= 0) {
-            const long long q = I.p_exy + (long long)(i + r) * I.npey + my;
-            const int c = tr.oy + lane;
-            const T psi = add_rn(mul_rn(a.bey[c], a.pExy[q]), mul_rn(a.cey[c], dA));
-            a.pExy[q] = psi;
-            e = add_rn(e, mul_rn(K[r], psi));
-            cx = add_rn(dA, psi);
-          }
+      Exo[id] = e;
+      e = ey[r];
+      if (i + r >= 1) {
+        const T dB = qdiv(sub_rn(hc, sH[r0 + r][lane + 1]), a.dx, a.rdx, a.fdx);
+        e = add_rn(ey[r], mul_rn(-dB, K[r]));
+        cy = -dB;
+        if (mxe[r] >= 0) {
+          const long long q = I.p_eyx + (long long)mxe[r] * tr.ny + j;
+          const int c = tr.ox + r0 + r;
+          const T psi = add_rn(mul_rn(a.bex[c], a.pEyx[q]), mul_rn(a.cex[c], dB));
+          a.pEyx[q] = psi;
+          e = add_rn(e, mul_rn(-K[r], psi));
+          cy = sub_rn(cy, psi);
         }
-        Exo[id] = e;
-        e = ey[r];
-        if (i + r >= 1) {
-          const T dB = qdiv(sub_rn(hc, sH[r0 + r][lane + 1]), a.dx, a.rdx, a.fdx);
-          e = add_rn(ey[r], mul_rn(-dB, K[r]));
-          cy = -dB;
-          if (mx[r] >= 0) {
-            const long long q = I.p_eyx + (long long)mx[r] * tr.ny + j;
-            const int c = tr.ox + r0 + r;
-            const T psi = add_rn(mul_rn(a.bex[c], a.pEyx[q]), mul_rn(a.cex[c], dB));
-            a.pEyx[q] = psi;
-            e = add_rn(e, mul_rn(-K[r], psi));
-            cy = sub_rn(cy, psi);
-          }
-        }
-        Eyo[id] = e;
-        const int di = r0 + r - tr.wdi, dj = lane - tr.wdj;
-        if (di >= 0 && di < tr.wdn && dj >= 0 && dj < tr.wdn) {
-          const long long slot = n % a.ring_len;
-          T* rr = a.ring + (slot * a.n_design + I.goff + (long long)di * tr.wdn + dj) * 2;
-          rr[0] = cx;
-          rr[1] = cy;
-        }
+      }
+      Eyo[id] = e;
+      const int di = r0 + r - tr.wdi, dj = lane - tr.wdj;
+      if (di >= 0 && di < tr.wdn && dj >= 0 && dj < tr.wdn) {
+        const long long slot = n % a.ring_len;
+        T* rr = a.ring + (slot * a.n_design + I.goff + (long long)di * tr.wdn + dj) * 2;
+        rr[0] = cx;
+        rr[1] = cy;
       }
     }
     __syncthreads();  // sH is rewritten by the next tile
@@ -689,10 +698,10 @@ __device__ __forceinline__ void adj_h_value(const BArgs<T>& a, const Inst& I, in
 }
 
 template <typename T, int R, bool HT, bool ET>
-__global__ void __launch_bounds__(32 * kWarps) kb_adj_step(const __grid_constant__ BArgs<T> a,
-                                                          const __grid_constant__ AArgs<T> d,
-                                                          int step_t) {
+__global__ void __launch_bounds__(32 * kWarps, PFB_MINB_ASTEP) kb_adj_step(
+    const __grid_constant__ BArgs<T> a, const __grid_constant__ AArgs<T> d, int step_t) {
   constexpr int TR = kWarps * R;
+  static_assert(TR <= 32, "the halo column is one warp's work");
   __shared__ T sA[TR + 1][33];  // hA: [1 + row][1 + column]; row 0 = halo row
   __shared__ T sB[TR + 1][33];  // hB: column 0 = halo column
   const long long n = *a.base + step_t;
@@ -717,10 +726,25 @@ __global__ void __launch_bounds__(32 * kWarps) kb_adj_step(const __grid_constant
     const int i = tr.i0 + r0, j = tr.j0 + lane;
     const bool jv = j < tr.ny;
     const long long id0 = tr.base + (long long)r0 * tr.pitch + lane;
+    // ---- loads, all before the barrier: the E adjoints and coefficients of
+    // the own cells, then (HT) their H-transpose inputs and the halo's
+    T lx[R], ly[R], K[R];
+    int mxe[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const bool ok = jv && i + r < tr.nx;
+      const long long id = id0 + (long long)r * tr.pitch;
+      lx[r] = ok ? d.aEx[id] : T(0);
+      ly[r] = ok ? d.aEy[id] : T(0);
+      if (ET) {
+        K[r] = ok ? a.ce[id] : T(0);
+        mxe[r] = ok ? a.mex[tr.ox + r0 + r] : -1;
+      }
+    }
+    const int mye = (ET && jv) ? a.mey[tr.oy + lane] : -1;
     if (HT) {
-      // ---- H transpose of the tile's own cells
       T ah[R], ga0[R], ga1[R], gb[R + 1];
-      int mx[R];
+      int mxh[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const bool ok = jv && i + r < tr.nx;
@@ -729,15 +753,44 @@ __global__ void __launch_bounds__(32 * kWarps) kb_adj_step(const __grid_constant
         ga0[r] = ok ? gA[id] : T(0);
         ga1[r] = (ok && j + 1 < tr.ny) ? gA[id + 1] : T(0);
         gb[r] = ok ? gB[id] : T(0);
-        mx[r] = ok ? a.mhx[tr.ox + r0 + r] : -1;
+        mxh[r] = ok ? a.mhx[tr.ox + r0 + r] : -1;
       }
       gb[R] = (jv && i + R < tr.nx) ? gB[id0 + (long long)R * tr.pitch] : T(0);
-      const int my = jv ? a.mhy[tr.oy + lane] : -1;
+      const int myh = jv ? a.mhy[tr.oy + lane] : -1;
+      // the halo cell of this thread, if any: warp 0 row i0 - 1 (its hA),
+      // warp 1 column j0 - 1 at tile row `lane` (its hB)
+      int hrole = 0, hi = 0, hj = 0, hcrow = 0, hccol = 0;
+      if (threadIdx.y == 0 && tr.i0 >= 1 && jv) {
+        hrole = 1;
+        hi = tr.i0 - 1;
+        hj = j;
+        hcrow = tr.ox - 1;
+        hccol = tr.oy + lane;
+      } else if (threadIdx.y == 1 && lane < TR && tr.j0 >= 1 && tr.i0 + lane < tr.nx) {
+        hrole = 2;
+        hi = tr.i0 + lane;
+        hj = tr.j0 - 1;
+        hcrow = tr.ox + lane;
+        hccol = tr.oy - 1;
+      }
+      T hah = T(0), hga0 = T(0), hga1 = T(0), hgb0 = T(0), hgb1 = T(0);
+      int hmx = -1, hmy = -1;
+      if (hrole) {
+        const long long id = tr.base + (long long)(hi - tr.i0) * tr.pitch + (hj - tr.j0);
+        hah = aHz[id];
+        hga0 = gA[id];
+        hga1 = hj + 1 < tr.ny ? gA[id + 1] : T(0);
+        hgb0 = gB[id];
+        hgb1 = hi + 1 < tr.nx ? gB[id + tr.pitch] : T(0);
+        hmx = a.mhx[hcrow];
+        hmy = a.mhy[hccol];
+      }
+      // ---- H transpose of the own cells
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         T h = T(0), ha = T(0), hb = T(0);
         if (jv && i + r < tr.nx) {
-          adj_h_value<T>(a, I, i + r, j, tr.nx, tr.ny, tr.ox + r0 + r, tr.oy + lane, mx[r], my,
+          adj_h_value<T>(a, I, i + r, j, tr.nx, tr.ny, tr.ox + r0 + r, tr.oy + lane, mxh[r], myh,
                          ah[r], ga0[r], ga1[r], gb[r], gb[r + 1], pzx, pzxo, pzy, pzyo, h, ha,
                          hb);
           aHzo[id0 + (long long)r * tr.pitch] = h;
@@ -745,104 +798,70 @@ __global__ void __launch_bounds__(32 * kWarps) kb_adj_step(const __grid_constant
         sA[r0 + r + 1][lane + 1] = ha;
         sB[r0 + r + 1][lane + 1] = hb;
       }
-      // ---- halo row i0 - 1 (warp 0): its hA, recomputed from the read level
-      if (threadIdx.y == 0) {
-        T ha = T(0);
-        if (tr.i0 >= 1 && jv) {
-          const long long id = tr.base - tr.pitch + lane;
-          T h, hb;
-          adj_h_value<T>(a, I, tr.i0 - 1, j, tr.nx, tr.ny, tr.ox - 1, tr.oy + lane,
-                         a.mhx[tr.ox - 1], a.mhy[tr.oy + lane], aHz[id], gA[id],
-                         j + 1 < tr.ny ? gA[id + 1] : T(0), gB[id], gB[id + tr.pitch], pzx,
-                         nullptr, pzy, nullptr, h, ha, hb);
-        }
-        sA[0][lane + 1] = ha;
-      }
-      // ---- halo column j0 - 1 (lanes 0 .. R-1 of each warp): its hB
-      if (lane < R) {
-        const int ih = i + lane;
-        T hb = T(0);
-        if (tr.j0 >= 1 && ih < tr.nx) {
-          const long long id = tr.base + (long long)(r0 + lane) * tr.pitch - 1;
-          T h, ha;
-          adj_h_value<T>(a, I, ih, tr.j0 - 1, tr.nx, tr.ny, tr.ox + r0 + lane, tr.oy - 1,
-                         a.mhx[tr.ox + r0 + lane], a.mhy[tr.oy - 1], aHz[id], gA[id],
-                         gA[id + 1], gB[id], ih + 1 < tr.nx ? gB[id + tr.pitch] : T(0), pzx,
-                         nullptr, pzy, nullptr, h, ha, hb);
-        }
-        sB[r0 + lane + 1][0] = hb;
+      // ---- the halo cell, recomputed from the read level (psi not stored)
+      {
+        T h = T(0), ha = T(0), hb = T(0);
+        if (hrole)
+          adj_h_value<T>(a, I, hi, hj, tr.nx, tr.ny, hcrow, hccol, hmx, hmy, hah, hga0, hga1,
+                         hgb0, hgb1, pzx, nullptr, pzy, nullptr, h, ha, hb);
+        if (threadIdx.y == 0) sA[0][lane + 1] = hrole == 1 ? ha : T(0);
+        if (threadIdx.y == 1 && lane < TR) sB[lane + 1][0] = hrole == 2 ? hb : T(0);
       }
       __syncthreads();
     }
     // ---- E adjoints: finish step n's (HT), then the E transpose of step m (ET)
-    {
-      T lx[R], ly[R], K[R];
-      int mx[R];
 #pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const bool ok = jv && i + r < tr.nx;
-        const long long id = id0 + (long long)r * tr.pitch;
-        lx[r] = ok ? d.aEx[id] : T(0);
-        ly[r] = ok ? d.aEy[id] : T(0);
-        if (ET) {
-          K[r] = ok ? a.ce[id] : T(0);
-          mx[r] = ok ? a.mex[tr.ox + r0 + r] : -1;
-        }
+    for (int r = 0; r < R; ++r) {
+      if (!(jv && i + r < tr.nx)) break;
+      const long long id = id0 + (long long)r * tr.pitch;
+      T x = lx[r], y = ly[r];
+      if (HT) {
+        y = fma_rn(sub_rn(sA[r0 + r][lane + 1], sA[r0 + r + 1][lane + 1]), a.idx, y);
+        x = fma_rn(sub_rn(sB[r0 + r + 1][lane], sB[r0 + r + 1][lane + 1]), a.idy, x);
       }
-      const int my = (ET && jv) ? a.mey[tr.oy + lane] : -1;
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        if (!(jv && i + r < tr.nx)) break;
-        const long long id = id0 + (long long)r * tr.pitch;
-        T x = lx[r], y = ly[r];
-        if (HT) {
-          y = fma_rn(sub_rn(sA[r0 + r][lane + 1], sA[r0 + r + 1][lane + 1]), a.idx, y);
-          x = fma_rn(sub_rn(sB[r0 + r + 1][lane], sB[r0 + r + 1][lane + 1]), a.idy, x);
+      if (ET) {
+        if (i + r == I.line_i) {
+          const double* ph = d.phase + m * d.n_freq * 2;
+          const double* g = d.cot + (I.loff + j) * d.n_freq * 2;
+          double sum = 0.0;
+          for (int f = 0; f < d.n_freq; ++f)
+            sum = __dadd_rn(sum, __dadd_rn(__dmul_rn(g[2 * f], ph[2 * f]),
+                                           __dmul_rn(g[2 * f + 1], ph[2 * f + 1])));
+          y = (T)__dadd_rn((double)y, __dmul_rn(d.dt, sum));
         }
-        if (ET) {
-          if (i + r == I.line_i) {
-            const double* ph = d.phase + m * d.n_freq * 2;
-            const double* g = d.cot + (I.loff + j) * d.n_freq * 2;
-            double sum = 0.0;
-            for (int f = 0; f < d.n_freq; ++f)
-              sum = __dadd_rn(sum, __dadd_rn(__dmul_rn(g[2 * f], ph[2 * f]),
-                                             __dmul_rn(g[2 * f + 1], ph[2 * f + 1])));
-            y = (T)__dadd_rn((double)y, __dmul_rn(d.dt, sum));
-          }
-          const int di = r0 + r - tr.wdi, dj = lane - tr.wdj;
-          if (di >= 0 && di < tr.wdn && dj >= 0 && dj < tr.wdn) {
-            const long long dc = I.goff + (long long)di * tr.wdn + dj;
-            const T* rr = a.ring + ((m % a.ring_len) * a.n_design + dc) * 2;
-            d.grad[dc] = __dadd_rn(d.grad[dc], __dadd_rn(__dmul_rn((double)x, (double)rr[0]),
-                                                         __dmul_rn((double)y, (double)rr[1])));
-          }
-          T ga = T(0), gbv = T(0);
-          if (j >= 1) {
-            ga = mul_rn(K[r], x);
-            if (my >= 0) {
-              const long long q = I.p_exy + (long long)(i + r) * I.npey + my;
-              const int c = tr.oy + lane;
-              const T ap = fma_rn(K[r], x, d.aExy[q]);
-              ga = fma_rn(a.cey[c], ap, ga);
-              d.aExy[q] = mul_rn(a.bey[c], ap);
-            }
-          }
-          if (i + r >= 1) {
-            gbv = mul_rn(-K[r], y);
-            if (mx[r] >= 0) {
-              const long long q = I.p_eyx + (long long)mx[r] * tr.ny + j;
-              const int c = tr.ox + r0 + r;
-              const T ap = fma_rn(-K[r], y, d.aEyx[q]);
-              gbv = fma_rn(a.cex[c], ap, gbv);
-              d.aEyx[q] = mul_rn(a.bex[c], ap);
-            }
-          }
-          gAo[id] = ga;
-          gBo[id] = gbv;
+        const int di = r0 + r - tr.wdi, dj = lane - tr.wdj;
+        if (di >= 0 && di < tr.wdn && dj >= 0 && dj < tr.wdn) {
+          const long long dc = I.goff + (long long)di * tr.wdn + dj;
+          const T* rr = a.ring + ((m % a.ring_len) * a.n_design + dc) * 2;
+          d.grad[dc] = __dadd_rn(d.grad[dc], __dadd_rn(__dmul_rn((double)x, (double)rr[0]),
+                                                       __dmul_rn((double)y, (double)rr[1])));
         }
-        d.aEx[id] = x;
-        d.aEy[id] = y;
+        T ga = T(0), gbv = T(0);
+        if (j >= 1) {
+          ga = mul_rn(K[r], x);
+          if (mye >= 0) {
+            const long long q = I.p_exy + (long long)(i + r) * I.npey + mye;
+            const int c = tr.oy + lane;
+            const T ap = fma_rn(K[r], x, d.aExy[q]);
+            ga = fma_rn(a.cey[c], ap, ga);
+            d.aExy[q] = mul_rn(a.bey[c], ap);
+          }
+        }
+        if (i + r >= 1) {
+          gbv = mul_rn(-K[r], y);
+          if (mxe[r] >= 0) {
+            const long long q = I.p_eyx + (long long)mxe[r] * tr.ny + j;
+            const int c = tr.ox + r0 + r;
+            const T ap = fma_rn(-K[r], y, d.aEyx[q]);
+            gbv = fma_rn(a.cex[c], ap, gbv);
+            d.aEyx[q] = mul_rn(a.bex[c], ap);
+          }
+        }
+        gAo[id] = ga;
+        gBo[id] = gbv;
       }
+      d.aEx[id] = x;
+      d.aEy[id] = y;
     }
     if (HT) __syncthreads();  // sA / sB are rewritten by the next tile
   }

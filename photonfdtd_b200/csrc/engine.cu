@@ -521,13 +521,6 @@ int scan_finite(pf_engine* e) {
 
 template <typename T>
 void launch_h_split(pf_engine* e, const StepArgs<T>& a, dim3 g, dim3 b) {
-  if constexpr (std::is_same<T, float>::value) {
-    if (PFB_H_ROWS == 2 && b.x == 32 && b.y == 8) {  // 3D: two rows per thread, packed
-      g.y = (e->ny + 15) / 16;
-      k_h_split2<<<g, b, 0, e->stream>>>(a);
-      return;
-    }
-  }
   k_h_split<T><<<g, b, 0, e->stream>>>(a);
 }
 

@@ -17,9 +17,6 @@
 #pragma once
 
 #include "cell3d.cuh"
-#include "packed2.cuh"
-
-#include <type_traits>
 
 // Minimum resident 256-thread blocks per SM the split passes are compiled
 // for (register budget 65536 / (256 * n)). Measured on config 3 (384^3 ADE):
@@ -31,17 +28,6 @@
 #endif
 #ifndef PFB_MINB_E
 #define PFB_MINB_E 5
-#endif
-// Two-row packed H pass (k_h_split2) for float32 3D grids: 1 enables it.
-#ifndef PFB_H_ROWS
-#define PFB_H_ROWS 2
-#endif
-#ifndef PFB_MINB_H2
-#define PFB_MINB_H2 6
-#endif
-// Packed FP32 pairs inside one cell in the float32 E pass's bulk path.
-#ifndef PFB_E_PAIR
-#define PFB_E_PAIR 1
 #endif
 
 namespace pfb {
@@ -73,31 +59,6 @@ __device__ __forceinline__ void bulk3(const StepArgs<T>& a, const T f[3], const 
   }
 #pragma unroll
   for (int c = 0; c < 3; ++c) out[c] = bulk(f[c], K[c], q[2 * c], q[2 * c + 1]);
-}
-
-// bulk3 for one float32 cell of a 3D grid (divisor axes {1,2,2,0,0,1}) on
-// the packed FP32 instructions: the six divisions as three lane pairs,
-// (n0, n2) by (dy, dz), (n1, n3) by (dz, dx), (n4, n5) by (dx, dy), and the
-// first two components' updates as one pair. Same operations, same order,
-// same fast-path test as bulk3, so the same bits.
-__device__ __forceinline__ void bulk3_pair(const StepArgs<float>& a, const float f[3],
-                                           const float K[3], const float n[6], float out[3]) {
-  const float m = absmax(absmax(n[0], n[1]), absmax(absmax(n[2], n[3]), absmax(n[4], n[5])));
-  if (!(a.fdx && a.fdy && a.fdz && qdiv_ok(m))) {
-    const int ax[6] = {1, 2, 2, 0, 0, 1};
-    bulk3<float>(a, f, K, n, ax, out);
-    return;
-  }
-  const float2 qA = qdiv_fast2v(make_float2(n[0], n[2]), make_float2(a.dy, a.dz),
-                                make_float2(a.rdy, a.rdz));
-  const float2 qB = qdiv_fast2v(make_float2(n[1], n[3]), make_float2(a.dz, a.dx),
-                                make_float2(a.rdz, a.rdx));
-  const float2 qC = qdiv_fast2v(make_float2(n[4], n[5]), make_float2(a.dx, a.dy),
-                                make_float2(a.rdx, a.rdy));
-  const float2 o = bulk2(make_float2(f[0], f[1]), make_float2(K[0], K[1]), qA, qB);
-  out[0] = o.x;
-  out[1] = o.y;
-  out[2] = bulk(f[2], K[2], qC.x, qC.y);
 }
 
 __device__ __forceinline__ bool in_box(int i, int j0, int j1, int k0, int k1, const int* b0,
@@ -160,71 +121,6 @@ __global__ void __launch_bounds__(256, PFB_MINB_H) k_h_split(const __grid_consta
   h_cell<T>(a, i, j, k, box);
 }
 
-// The H pass of 3D float32 grids with two adjacent rows (j, j+1) per thread:
-// a 32 x 8 block covers 32 x 16 cells. In the bulk box the two cells' values
-// travel as float2 pairs through the packed FP32 instructions (packed2.cuh),
-// which round each cell as the scalar path does; row j reuses row j+1's own
-// Ez and Ex as its +y neighbours. Elsewhere (and when a numerator leaves the
-// fast division's range) each cell takes the scalar path.
-__global__ void __launch_bounds__(256, PFB_MINB_H2) k_h_split2(const __grid_constant__ StepArgs<float> a) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j0 = (blockIdx.y * blockDim.y + threadIdx.y) * 2;
-  const int i = blockIdx.z;
-  const bool box = in_box(i, blockIdx.y * blockDim.y * 2, (blockIdx.y + 1) * blockDim.y * 2,
-                          blockIdx.x * blockDim.x, (blockIdx.x + 1) * blockDim.x, a.hb0, a.hb1);
-  if (k >= a.nz || j0 >= a.ny) return;
-  if (!box) {
-    h_cell<float>(a, i, j0, k, false);
-    if (j0 + 1 < a.ny) h_cell<float>(a, i, j0 + 1, k, false);
-    return;
-  }
-  const long long sy = a.nz, sx = (long long)a.ny * a.nz;
-  const long long id0 = i * sx + j0 * sy + k, id1 = id0 + sy;
-  const float2 ex = make_float2(a.Ein[0][id0], a.Ein[0][id1]);
-  const float2 ey = make_float2(a.Ein[1][id0], a.Ein[1][id1]);
-  const float2 ez = make_float2(a.Ein[2][id0], a.Ein[2][id1]);
-  const float2 f0 = make_float2(a.Hin[0][id0], a.Hin[0][id1]);
-  const float2 f1 = make_float2(a.Hin[1][id0], a.Hin[1][id1]);
-  const float2 f2 = make_float2(a.Hin[2][id0], a.Hin[2][id1]);
-  // Hx: +dEz/dy - dEy/dz; Hy: +dEx/dz - dEz/dx; Hz: +dEy/dx - dEx/dy
-  const float2 n0 = sub2(make_float2(ez.y, a.Ein[2][id1 + sy]), ez);
-  const float2 n1 = sub2(make_float2(a.Ein[1][id0 + 1], a.Ein[1][id1 + 1]), ey);
-  const float2 n2 = sub2(make_float2(a.Ein[0][id0 + 1], a.Ein[0][id1 + 1]), ex);
-  const float2 n3 = sub2(make_float2(a.Ein[2][id0 + sx], a.Ein[2][id1 + sx]), ez);
-  const float2 n4 = sub2(make_float2(a.Ein[1][id0 + sx], a.Ein[1][id1 + sx]), ey);
-  const float2 n5 = sub2(make_float2(ex.y, a.Ein[0][id1 + sy]), ex);
-  const float m = fmaxf(fmaxf(absmax2(n0, n1), absmax2(n2, n3)), absmax2(n4, n5));
-  if (!(a.fdx && a.fdy && a.fdz && qdiv_ok(m))) {
-    // a numerator outside the fast division's range: the scalar path
-    const float nn[2][6] = {{n0.x, n1.x, n2.x, n3.x, n4.x, n5.x},
-                            {n0.y, n1.y, n2.y, n3.y, n4.y, n5.y}};
-    const float ff[2][3] = {{f0.x, f1.x, f2.x}, {f0.y, f1.y, f2.y}};
-    const float mch = -a.ch;
-    const float K[3] = {mch, mch, mch};
-    const int ax[6] = {1, 2, 2, 0, 0, 1};
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      float h[3];
-      bulk3<float>(a, ff[r], K, nn[r], ax, h);
-      const long long id = r ? id1 : id0;
-      a.Hout[0][id] = h[0];
-      a.Hout[1][id] = h[1];
-      a.Hout[2][id] = h[2];
-    }
-    return;
-  }
-  const float2 K = bc2(-a.ch);
-  const float2 h0 = bulk2(f0, K, qdiv_fast2(n0, a.dy, a.rdy), qdiv_fast2(n1, a.dz, a.rdz));
-  const float2 h1 = bulk2(f1, K, qdiv_fast2(n2, a.dz, a.rdz), qdiv_fast2(n3, a.dx, a.rdx));
-  const float2 h2 = bulk2(f2, K, qdiv_fast2(n4, a.dx, a.rdx), qdiv_fast2(n5, a.dy, a.rdy));
-  a.Hout[0][id0] = h0.x;
-  a.Hout[0][id1] = h0.y;
-  a.Hout[1][id0] = h1.x;
-  a.Hout[1][id1] = h1.y;
-  a.Hout[2][id0] = h2.x;
-  a.Hout[2][id1] = h2.y;
-}
-
 // E pass: E^{n+1} = E^n + ce (curl H^{n+1/2} + psi), then ADE.
 template <typename T, int CE, bool ADE>
 __global__ void __launch_bounds__(256, PFB_MINB_E) k_e_split(const __grid_constant__ StepArgs<T> a) {
@@ -233,6 +129,7 @@ __global__ void __launch_bounds__(256, PFB_MINB_E) k_e_split(const __grid_consta
   const int i = blockIdx.z;
   const bool box = in_box(i, blockIdx.y * blockDim.y, (blockIdx.y + 1) * blockDim.y,
                           blockIdx.x * blockDim.x, (blockIdx.x + 1) * blockDim.x, a.eb0, a.eb1);
+  const MediumT<T>* media = a.media;
   if (k >= a.nz || j >= a.ny) return;
   const long long sy = a.nz, sx = (long long)a.ny * a.nz;
   const long long id = i * sx + j * sy + k;
@@ -262,21 +159,17 @@ __global__ void __launch_bounds__(256, PFB_MINB_E) k_e_split(const __grid_consta
     hn[4] = ld_if(a.Hin[1], id, -sx, lx);
     hn[5] = ld_if(a.Hin[0], id, -sy, ly);
   }
-  cell_decode<T, CE, ADE>(a, a.media, t, K, w);
+  cell_decode<T, CE, ADE>(a, media, t, K, w);
   AdeRec<T> rec;
-  if (ADE && w) ade_load<T>(a, a.media, w, rec);
+  if (ADE && w) ade_load<T>(a, media, w, rec);
   T e[3];
   if (box || d3) {
     // Ex: +dHz/dy - dHy/dz; Ey: +dHx/dz - dHz/dx; Ez: +dHy/dx - dHx/dy
     const T n[6] = {sub_rn(hz, hn[0]), sub_rn(hy, hn[1]), sub_rn(hx, hn[2]),
                     sub_rn(hz, hn[3]), sub_rn(hy, hn[4]), sub_rn(hx, hn[5])};
     if (box) {
-      if constexpr (std::is_same<T, float>::value && PFB_E_PAIR) {
-        bulk3_pair(a, en, K, n, e);
-      } else {
-        const int ax[6] = {1, 2, 2, 0, 0, 1};
-        bulk3<T>(a, en, K, n, ax, e);
-      }
+      const int ax[6] = {1, 2, 2, 0, 0, 1};
+      bulk3<T>(a, en, K, n, ax, e);
     } else {
       e3<T>(a, i, j, k, en, K, n, e);
     }
@@ -289,7 +182,7 @@ __global__ void __launch_bounds__(256, PFB_MINB_E) k_e_split(const __grid_consta
     e[2] = upd_ez<T>(a, i, j, k, en[2], K[2], hy, ld_if(a.Hin[1], id, -sx, lx), hx,
                      ld_if(a.Hin[0], id, -sy, ly));
   }
-  if (ADE && w) ade_update<T>(a, a.media, rec, en, e);
+  if (ADE && w) ade_update<T>(a, media, rec, en, e);
   a.Eout[0][id] = e[0];
   a.Eout[1][id] = e[1];
   a.Eout[2][id] = e[2];
