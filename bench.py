@@ -389,6 +389,7 @@ def e2e_bench(size: int, steps: int, world: int, dist) -> dict:
             "d2h_bytes_per_step": int(st["d2h_bytes"] / steps),
             "steps": steps, "wall_s": round(wall, 3),
             "phases_s": {"tables": round(st["tables_s"], 3), "engine": round(st["create_s"], 3),
+                         "steps": round(st["advance_s"], 3),
                          "steps_and_readback": round(st["run_s"], 3)},
             "what": f"{api}: config 3 at {size}^3 for {steps} steps, host scene in, "
                     "Result (DFT + flux) out, wall clock"}

@@ -559,6 +559,7 @@ def run_b200(sim, kernel: int = N.PF_KERNEL_AUTO):
     t3 = time.perf_counter()
     LAST_RUN.clear()
     LAST_RUN.update(tables_s=t1 - t0, create_s=t2 - t1, run_s=t3 - t2,
+                    advance_s=LAST_STEPPING_S[0],
                     h2d_bytes=upload_bytes(t), n_steps=t["n_steps"],
                     d2h_bytes=result_bytes(res), cells=int(np.prod(t["shape"])))
     if getattr(sim, "b200_error_vs_f64", False) and np.dtype(t["npdt"]) != np.float64:
@@ -571,6 +572,7 @@ def run_b200(sim, kernel: int = N.PF_KERNEL_AUTO):
 # building the tables on the host, creating the engine (device allocation and
 # upload), stepping with monitor read-back.
 LAST_RUN: Dict[str, float] = {}
+LAST_STEPPING_S = [0.0]  # time inside pf_advance during the last drive()
 
 
 def upload_bytes(t) -> int:
@@ -632,11 +634,16 @@ def drive(sim, eng: B200Engine, t: dict, mon_dtype=None):
     every = max(n_steps // 100, 1)
     pos = 0
 
+    import time
+    stepping = [0.0]
+
     def advance_to(end):
         nonlocal pos
         while pos < end:
             n = min(end - pos, every) if cb is not None else end - pos
+            t0 = time.perf_counter()
             eng.advance(pos, n)
+            stepping[0] += time.perf_counter() - t0
             pos += n
             if cb is not None:
                 cb(min(pos, n_steps), n_steps)
@@ -676,4 +683,5 @@ def drive(sim, eng: B200Engine, t: dict, mon_dtype=None):
                               for c in m.components}
     for k, f in enumerate(t["flux"]):
         result.flux[f["m"].name] = eng.read_flux(k)
+    LAST_STEPPING_S[0] = stepping[0]
     return result
