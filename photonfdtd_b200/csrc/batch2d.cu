@@ -73,6 +73,10 @@ struct pf_batch {
   std::vector<void*> allocs;
   Inst* d_inst = nullptr;
   TileRec* d_tiles = nullptr;
+  SegRec* d_segs = nullptr;   // marching segments (forward step)
+  int nsegs = 0;
+  size_t seg_cap = 0;         // SegRec slots of d_segs (the shortest segments)
+  bool march = true;          // forward step: marching warps (else kb_step tiles)
   int ntiles = 0;
   int tile_rows = 32;
   size_t tile_cap = 0;  // TileRec slots of d_tiles (the 8-row list, the longest)
@@ -153,6 +157,8 @@ BArgs<T> bargs(pf_batch* b) {
   memset(&a, 0, sizeof a);
   a.inst = b->d_inst;
   a.tiles = b->d_tiles;
+  a.segs = b->d_segs;
+  a.nsegs = b->nsegs;
   a.ntiles = b->ntiles;
   a.Ex = (T*)b->Ex;
   a.Ey = (T*)b->Ey;
@@ -245,7 +251,11 @@ void fwd_kernels(pf_batch* b, long long len, bool dft) {
   const long long ng = b->src.n_groups;
   int pend = 0;
   for (long long t = 0; t < len; ++t) {
-    if (b->fused) {
+    if (b->fused && b->march) {
+      kb_march<T><<<(unsigned)((b->nsegs + kMarchWarps - 1) / kMarchWarps), dim3(32, kMarchWarps),
+                    0, b->stream>>>(a, (int)t);
+      b->capture_launches += 1;
+    } else if (b->fused) {
       kb_step<T, R><<<G, blk, 0, b->stream>>>(a, (int)t);
       b->capture_launches += 1;
     } else {
@@ -303,6 +313,18 @@ void adj_kernels(pf_batch* b, long long len) {
   const AArgs<T> d = aargs<T>(b);
   const dim3 blk(32, kWarps);
   const int G = grid_blocks(b);
+  if (b->fused && b->march) {
+    const dim3 mg((unsigned)((b->nsegs + kMarchWarps - 1) / kMarchWarps)), mb(32, kMarchWarps);
+    kb_adj_march<T, false, true><<<mg, mb, 0, b->stream>>>(a, d, (int)(len - 1));
+    for (long long t = len - 1; t >= 0; --t) {
+      if (t > 0)
+        kb_adj_march<T, true, true><<<mg, mb, 0, b->stream>>>(a, d, (int)t);
+      else
+        kb_adj_march<T, true, false><<<mg, mb, 0, b->stream>>>(a, d, 0);
+    }
+    b->capture_launches += 1 + len;
+    return;
+  }
   if (b->fused) {
     kb_adj_step<T, R, false, true><<<G, blk, 0, b->stream>>>(a, d, (int)(len - 1));
     for (long long t = len - 1; t >= 0; --t) {
@@ -619,12 +641,37 @@ std::vector<TileRec> make_tiles(const pf_batch* b, int tile_rows) {
   return tiles;
 }
 
+// The marching segments at a height of seg_rows rows: every instance's
+// strips of 31 owned columns, each cut into row ranges.
+std::vector<SegRec> make_segs(const pf_batch* b, int seg_rows) {
+  std::vector<SegRec> segs;
+  for (int k = 0; k < b->n_inst; ++k) {
+    const Inst& I = b->inst[k];
+    for (int j0 = 0; j0 < I.ny; j0 += kMarchCols)
+      for (int i0 = 0; i0 < I.nx; i0 += seg_rows) {
+        SegRec sg;
+        sg.k = k;
+        sg.i0 = i0;
+        sg.i1 = std::min(I.nx, i0 + seg_rows);
+        sg.j0 = j0;
+        segs.push_back(sg);
+      }
+  }
+  return segs;
+}
+
 int set_tile_rows(pf_batch* b, int tile_rows) {
   const std::vector<TileRec> tiles = make_tiles(b, tile_rows);
   if (tiles.size() > b->tile_cap) return bfail(b, PF_ERR_INVALID, "tile list exceeds its buffer");
   B_CUDA(b, cudaMemcpyAsync(b->d_tiles, tiles.data(), tiles.size() * sizeof(TileRec),
                             cudaMemcpyHostToDevice, b->stream));
-  B_CUDA(b, cudaStreamSynchronize(b->stream));  // before `tiles` goes
+  // the marching steps' segments are 2 x tile_rows rows high
+  const std::vector<SegRec> segs = make_segs(b, 2 * tile_rows);
+  if (segs.size() > b->seg_cap) return bfail(b, PF_ERR_INVALID, "segment list exceeds its buffer");
+  B_CUDA(b, cudaMemcpyAsync(b->d_segs, segs.data(), segs.size() * sizeof(SegRec),
+                            cudaMemcpyHostToDevice, b->stream));
+  b->nsegs = (int)segs.size();
+  B_CUDA(b, cudaStreamSynchronize(b->stream));  // before `tiles` and `segs` go
   destroy_graphs(b);  // captured with the old grid and row count
   b->ntiles = (int)tiles.size();
   b->rows = tile_rows / kWarps;
@@ -774,6 +821,17 @@ int pfb_finalize(pf_batch* b, int checkpoint_every, int tile_rows) {
   if ((rc = balloc(b, (void**)&b->d_tiles, b->tile_cap * sizeof(TileRec)))) return rc;
   B_CUDA(b, cudaMemcpyAsync(b->d_tiles, tiles.data(), tiles.size() * sizeof(TileRec),
                             cudaMemcpyHostToDevice, b->stream));
+  {
+    const std::vector<SegRec> segs = make_segs(b, 2 * tile_rows);
+    b->seg_cap = make_segs(b, 16).size();
+    if ((long long)b->seg_cap >= (1LL << 31)) return bfail(b, PF_ERR_INVALID, "too many segments");
+    b->nsegs = (int)segs.size();
+    if ((rc = balloc(b, (void**)&b->d_segs, b->seg_cap * sizeof(SegRec)))) return rc;
+    B_CUDA(b, cudaMemcpyAsync(b->d_segs, segs.data(), segs.size() * sizeof(SegRec),
+                              cudaMemcpyHostToDevice, b->stream));
+    B_CUDA(b, cudaStreamSynchronize(b->stream));
+    b->march = !getenv("PFB200_BATCH_TILESTEP");
+  }
   if ((rc = bup(b, &b->ce, cep.data(), cep.size()))) return rc;
   for (int q = 0; q < 8; ++q)
     if ((rc = bup(b, &b->coef[q], coefp[q].data(), coefp[q].size()))) return rc;

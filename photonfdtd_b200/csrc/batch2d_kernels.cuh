@@ -29,6 +29,10 @@ constexpr int kWarps = 8;     // warps per block
 #ifndef PFB_MINB_ASTEP
 #define PFB_MINB_ASTEP 4
 #endif
+// Minimum resident 128-thread blocks per SM of the marching forward step.
+#ifndef PFB_MINB_MARCH
+#define PFB_MINB_MARCH 10
+#endif
 constexpr int kDftRing = 32;  // line samples kept before a DFT flush
 
 struct Inst {
@@ -54,11 +58,21 @@ struct __align__(16) TileRec {
   int pad[1];
 };
 
+// A marching segment: instance k, rows [i0, i1), owned columns [j0, j0 + 31).
+// Its warp's lane l holds column j0 - 1 + l: lane 0 is the halo column.
+struct SegRec {
+  int k, i0, i1, j0;
+};
+constexpr int kMarchCols = 31;  // owned columns per warp
+constexpr int kMarchWarps = 4;  // warps (segments) per block
+
 template <typename T>
 struct BArgs {
   const Inst* inst;
   const TileRec* tiles;
   int ntiles;
+  const SegRec* segs;
+  int nsegs;
   T *Ex, *Ey, *Hz;
   const T* ce;
   const T *bex, *cex, *bhx, *chx, *bey, *cey, *bhy, *chy;
@@ -390,6 +404,143 @@ __global__ void __launch_bounds__(32 * kWarps, PFB_MINB_STEP) kb_step(
       }
     }
     __syncthreads();  // sH is rewritten by the next tile
+  }
+}
+
+// ---- marching forward step ---------------------------------------------------
+// One warp per segment marches down its rows: lane l holds column
+// j0 - 1 + l, so the left neighbour of every owned column (lanes 1..31) sits
+// in the lane below and the right neighbour in the lane above (shuffles);
+// lane 0 is a halo column whose Hz it recomputes without storing, and lane 31
+// loads the one Ex beyond the strip. The Hz of the previous row stays in a
+// register; a segment that starts below row 0 first recomputes its row
+// i0 - 1 (Hz only). The next row's loads are issued before the current row is
+// computed. As in kb_step, level n & 1 is read and level (n & 1) ^ 1
+// written, so segments never race, and every cell's arithmetic is kb_h's and
+// kb_e's (hz_value and the E update below), bit for bit. No shared memory,
+// no barriers, about four cell loads and three stores per cell and step.
+template <typename T>
+__global__ void __launch_bounds__(32 * kMarchWarps, PFB_MINB_MARCH) kb_march(
+    const __grid_constant__ BArgs<T> a, int step_t) {
+  const int w = blockIdx.x * kMarchWarps + threadIdx.y;
+  if (w >= a.nsegs) return;  // uniform over the warp
+  const SegRec sg = a.segs[w];
+  const Inst& I = a.inst[sg.k];
+  const long long n = *a.base + step_t;
+  const int L = (int)(n & 1);
+  const T* Ex = a.Ex2[L];
+  const T* Ey = a.Ey2[L];
+  const T* Hz = a.Hz2[L];
+  T* Exo = a.Ex2[L ^ 1];
+  T* Eyo = a.Ey2[L ^ 1];
+  T* Hzo = a.Hz2[L ^ 1];
+  const T* pzx = a.pHzx2[L];
+  const T* pzy = a.pHzy2[L];
+  T* pzxo = a.pHzx2[L ^ 1];
+  T* pzyo = a.pHzy2[L ^ 1];
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x;
+  const int nx = I.nx, ny = I.ny;
+  const long long pitch = I.pitch;
+  const int j = sg.j0 - 1 + lane;
+  const bool jv = j >= 0 && j < ny;
+  const bool own = lane >= 1 && jv;
+  const bool hcol = jv && j < ny - 1;       // Hz is updated in this column
+  const bool xr = lane == 31 && j + 1 < ny;  // lane 31 loads Ex one column right
+  const long long c0 = I.off + j;           // pooled index of (0, j)
+  const int myh = jv ? a.mhy[I.oy + j] : -1;
+  const int mye = jv ? a.mey[I.oy + j] : -1;
+  const int slot = (int)(n % a.ring_len);
+  const int r_first = sg.i0 > 0 ? sg.i0 - 1 : 0;
+  // row r_first
+  T ex = T(0), hz = T(0), ey = T(0), eyn = T(0), K = T(0), ex31 = T(0);
+  {
+    const long long id = c0 + r_first * pitch;
+    if (jv) {
+      ex = Ex[id];
+      hz = Hz[id];
+      ey = Ey[id];
+      if (r_first + 1 < nx) eyn = Ey[id + pitch];
+      if (r_first >= sg.i0) K = a.ce[id];
+    }
+    if (xr) ex31 = Ex[id + 1];
+  }
+  T hz_prev = T(0);  // Hz^{n+1/2} of the row above
+  for (int r = r_first; r < sg.i1; ++r) {
+    // the next row's loads first
+    const int r1 = r + 1;
+    T ex_n = T(0), hz_n = T(0), eyn_n = T(0), K_n = T(0), ex31_n = T(0);
+    if (r1 < sg.i1) {
+      const long long id = c0 + r1 * pitch;
+      if (jv) {
+        ex_n = Ex[id];
+        hz_n = Hz[id];
+        if (r1 + 1 < nx) eyn_n = Ey[id + pitch];
+        K_n = a.ce[id];
+      }
+      if (xr) ex31_n = Ex[id + 1];
+    }
+    const long long id = c0 + r * pitch;
+    const bool body = r >= sg.i0;  // uniform: a row this segment owns
+    // Hz of row r (every lane: the halo lane and the prologue row too)
+    T exr = __shfl_down_sync(full, ex, 1);
+    if (lane == 31) exr = ex31;
+    T h = hz;
+    if (hcol && r < nx - 1) {
+      const bool st = own && body;
+      h = hz_value<T>(a, I, r, j, ny, I.ox + r, I.oy + j, a.mhx[I.ox + r], myh, hz, eyn, ey,
+                      exr, ex, pzx, st ? pzxo : nullptr, pzy, st ? pzyo : nullptr);
+    }
+    const T hl = __shfl_up_sync(full, h, 1);  // Hz^{n+1/2} of column j - 1
+    if (body && own) {
+      Hzo[id] = h;
+      // Ex, Ey of (r, j): kb_e's arithmetic
+      T cx = T(0), cy = T(0);
+      T e = ex;
+      if (j >= 1) {
+        const T dA = qdiv(sub_rn(h, hl), a.dy, a.rdy, a.fdy);
+        e = add_rn(ex, mul_rn(dA, K));
+        cx = dA;
+        if (mye >= 0) {
+          const long long q = I.p_exy + (long long)r * I.npey + mye;
+          const int c = I.oy + j;
+          const T psi = add_rn(mul_rn(a.bey[c], a.pExy[q]), mul_rn(a.cey[c], dA));
+          a.pExy[q] = psi;
+          e = add_rn(e, mul_rn(K, psi));
+          cx = add_rn(dA, psi);
+        }
+      }
+      Exo[id] = e;
+      e = ey;
+      if (r >= 1) {
+        const T dB = qdiv(sub_rn(h, hz_prev), a.dx, a.rdx, a.fdx);
+        e = add_rn(ey, mul_rn(-dB, K));
+        cy = -dB;
+        const int mx = a.mex[I.ox + r];
+        if (mx >= 0) {
+          const long long q = I.p_eyx + (long long)mx * ny + j;
+          const int c = I.ox + r;
+          const T psi = add_rn(mul_rn(a.bex[c], a.pEyx[q]), mul_rn(a.cex[c], dB));
+          a.pEyx[q] = psi;
+          e = add_rn(e, mul_rn(-K, psi));
+          cy = sub_rn(cy, psi);
+        }
+      }
+      Eyo[id] = e;
+      const int di = r - I.di0, dj = j - I.dj0;
+      if (di >= 0 && di < I.dn && dj >= 0 && dj < I.dn) {
+        T* rr = a.ring + ((long long)slot * a.n_design + I.goff + (long long)di * I.dn + dj) * 2;
+        rr[0] = cx;
+        rr[1] = cy;
+      }
+    }
+    hz_prev = h;
+    ex = ex_n;
+    hz = hz_n;
+    ey = eyn;
+    eyn = eyn_n;
+    K = K_n;
+    ex31 = ex31_n;
   }
 }
 
@@ -864,6 +1015,163 @@ __global__ void __launch_bounds__(32 * kWarps, PFB_MINB_ASTEP) kb_adj_step(
       d.aEy[id] = y;
     }
     if (HT) __syncthreads();  // sA / sB are rewritten by the next tile
+  }
+}
+
+// ---- marching reverse step ---------------------------------------------------
+// kb_adj_step's work on kb_march's segments: one warp marches down its rows;
+// gA of the column to the right comes from the lane above (lane 31 loads
+// it), gB of the next row is loaded one row ahead, hA of the row above stays
+// in a register, and hB of the column to the left comes from the lane below
+// (lane 0 recomputes the halo column's H transpose without storing it). A
+// segment that starts below row 0 first recomputes hA of row i0 - 1. Same
+// levels and arithmetic as kb_adj_step, so the same bits.
+template <typename T, bool HT, bool ET>
+__global__ void __launch_bounds__(32 * kMarchWarps, PFB_MINB_MARCH) kb_adj_march(
+    const __grid_constant__ BArgs<T> a, const __grid_constant__ AArgs<T> d, int step_t) {
+  const int w = blockIdx.x * kMarchWarps + threadIdx.y;
+  if (w >= a.nsegs) return;  // uniform over the warp
+  const SegRec sg = a.segs[w];
+  const Inst& I = a.inst[sg.k];
+  const long long n = *a.base + step_t;
+  const long long m = HT ? n - 1 : n;  // the step of the E transpose
+  const int lg = (int)(n & 1);
+  const int lh = (int)((n + 1) & 1);
+  const T* gA = d.gA2[lg];
+  const T* gB = d.gB2[lg];
+  T* gAo = d.gA2[(int)(m & 1)];
+  T* gBo = d.gB2[(int)(m & 1)];
+  const T* aHz = d.aHz2[lh];
+  T* aHzo = d.aHz2[lh ^ 1];
+  const T* pzx = d.aHzx2[lh];
+  const T* pzy = d.aHzy2[lh];
+  T* pzxo = d.aHzx2[lh ^ 1];
+  T* pzyo = d.aHzy2[lh ^ 1];
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x;
+  const int nx = I.nx, ny = I.ny;
+  const long long pitch = I.pitch;
+  const int j = sg.j0 - 1 + lane;
+  const bool jv = j >= 0 && j < ny;
+  const bool own = lane >= 1 && jv;
+  const bool xr = HT && lane == 31 && j + 1 < ny;
+  const long long c0 = I.off + j;
+  const int myh = (HT && jv) ? a.mhy[I.oy + j] : -1;
+  const int mye = (ET && jv) ? a.mey[I.oy + j] : -1;
+  const int r_first = (HT && sg.i0 > 0) ? sg.i0 - 1 : sg.i0;
+  // row r_first
+  T ah = T(0), ga = T(0), ga31 = T(0), gb = T(0), gbn = T(0), lx = T(0), ly = T(0), K = T(0);
+  {
+    const long long id = c0 + r_first * pitch;
+    if (jv) {
+      if (HT) {
+        ah = aHz[id];
+        ga = gA[id];
+        gb = gB[id];
+        if (r_first + 1 < nx) gbn = gB[id + pitch];
+      }
+      if (r_first >= sg.i0) {
+        lx = d.aEx[id];
+        ly = d.aEy[id];
+        if (ET) K = a.ce[id];
+      }
+    }
+    if (xr) ga31 = gA[id + 1];
+  }
+  T ha_prev = T(0);  // hA of the row above
+  for (int r = r_first; r < sg.i1; ++r) {
+    const int r1 = r + 1;
+    T ah_n = T(0), ga_n = T(0), ga31_n = T(0), gbn_n = T(0), lx_n = T(0), ly_n = T(0), K_n = T(0);
+    if (r1 < sg.i1) {
+      const long long id = c0 + r1 * pitch;
+      if (jv) {
+        if (HT) {
+          ah_n = aHz[id];
+          ga_n = gA[id];
+          if (r1 + 1 < nx) gbn_n = gB[id + pitch];
+        }
+        lx_n = d.aEx[id];
+        ly_n = d.aEy[id];
+        if (ET) K_n = a.ce[id];
+      }
+      if (xr) ga31_n = gA[id + 1];
+    }
+    const long long id = c0 + r * pitch;
+    const bool body = r >= sg.i0;  // uniform
+    T ha = T(0), hb = T(0);
+    if (HT) {
+      T ga1 = __shfl_down_sync(full, ga, 1);
+      if (lane == 31) ga1 = ga31;
+      T h = T(0);
+      if (jv) {
+        const bool st = own && body;
+        adj_h_value<T>(a, I, r, j, nx, ny, I.ox + r, I.oy + j, a.mhx[I.ox + r], myh, ah, ga,
+                       ga1, gb, gbn, pzx, st ? pzxo : nullptr, pzy, st ? pzyo : nullptr, h, ha,
+                       hb);
+        if (st) aHzo[id] = h;
+      }
+    }
+    const T hbl = HT ? __shfl_up_sync(full, hb, 1) : T(0);  // hB of column j - 1
+    if (body && own) {
+      T x = lx, y = ly;
+      if (HT) {
+        y = fma_rn(sub_rn(ha_prev, ha), a.idx, y);
+        x = fma_rn(sub_rn(hbl, hb), a.idy, x);
+      }
+      if (ET) {
+        if (r == I.line_i) {
+          const double* ph = d.phase + m * d.n_freq * 2;
+          const double* g = d.cot + (I.loff + j) * d.n_freq * 2;
+          double sum = 0.0;
+          for (int f = 0; f < d.n_freq; ++f)
+            sum = __dadd_rn(sum, __dadd_rn(__dmul_rn(g[2 * f], ph[2 * f]),
+                                           __dmul_rn(g[2 * f + 1], ph[2 * f + 1])));
+          y = (T)__dadd_rn((double)y, __dmul_rn(d.dt, sum));
+        }
+        const int di = r - I.di0, dj = j - I.dj0;
+        if (di >= 0 && di < I.dn && dj >= 0 && dj < I.dn) {
+          const long long dc = I.goff + (long long)di * I.dn + dj;
+          const T* rr = a.ring + ((m % a.ring_len) * a.n_design + dc) * 2;
+          d.grad[dc] = __dadd_rn(d.grad[dc], __dadd_rn(__dmul_rn((double)x, (double)rr[0]),
+                                                       __dmul_rn((double)y, (double)rr[1])));
+        }
+        T gav = T(0), gbv = T(0);
+        if (j >= 1) {
+          gav = mul_rn(K, x);
+          if (mye >= 0) {
+            const long long q = I.p_exy + (long long)r * I.npey + mye;
+            const int c = I.oy + j;
+            const T ap = fma_rn(K, x, d.aExy[q]);
+            gav = fma_rn(a.cey[c], ap, gav);
+            d.aExy[q] = mul_rn(a.bey[c], ap);
+          }
+        }
+        if (r >= 1) {
+          gbv = mul_rn(-K, y);
+          const int mx = a.mex[I.ox + r];
+          if (mx >= 0) {
+            const long long q = I.p_eyx + (long long)mx * ny + j;
+            const int c = I.ox + r;
+            const T ap = fma_rn(-K, y, d.aEyx[q]);
+            gbv = fma_rn(a.cex[c], ap, gbv);
+            d.aEyx[q] = mul_rn(a.bex[c], ap);
+          }
+        }
+        gAo[id] = gav;
+        gBo[id] = gbv;
+      }
+      d.aEx[id] = x;
+      d.aEy[id] = y;
+    }
+    ha_prev = ha;
+    ah = ah_n;
+    ga = ga_n;
+    ga31 = ga31_n;
+    gb = gbn;
+    gbn = gbn_n;
+    lx = lx_n;
+    ly = ly_n;
+    K = K_n;
   }
 }
 
