@@ -185,6 +185,43 @@ int pf_get_state(pf_engine *eng, void *dst, int64_t bytes, int dst_on_device);
 int pf_set_state(pf_engine *eng, int64_t step, const void *src, int64_t bytes,
                  int src_on_device);
 
+/* Adjoint of the stepping: the gradient of a loss J of the monitor outputs
+ * with respect to the per-cell E coefficient K = dt / (eps0 eps_r), i.e. the
+ * time-domain adjoint behind value_and_grad_eps
+ * (src/photonfdtd/jaxbackend.py:666-722, which differentiates the same step
+ * with jax.grad; like it, no dispersive media and no subpixel tensor:
+ * PF_ERR_UNSUPPORTED). Protocol, after a forward run that saved pf_get_state
+ * checkpoints at the segment starts:
+ *   pf_adj_init(ring_steps)     adjoint state + a replay ring of ring_steps
+ *                               steps (the longest segment); zeroes the
+ *                               adjoint and the gradient
+ *   pf_adj_set_dft_cotangent(mon, cot)
+ *                               dJ/d(DFT accumulator) of monitor mon as
+ *                               (components in mask order, n_freq, region
+ *                               cells) complex128 interleaved, G = dJ/dRe +
+ *                               i dJ/dIm
+ *   pf_adj_add_field_source(step, comp, region, vals)
+ *                               dJ/d(field snapshot taken after step `step`,
+ *                               the FieldMonitor frame) over a strided region
+ *   pf_adj_segment(step0, n, state)
+ *                               for segments from the last to the first
+ *                               (step0 + n must be where the reverse pass
+ *                               stands: n_steps, then the previous step0):
+ *                               restores the checkpoint of step0, replays n
+ *                               steps recording H and psi_E (monitors not
+ *                               sampled), then runs their n reverse steps
+ *   pf_adj_read_grad(dst)       dJ/dK per cell, summed over Ex, Ey, Ez
+ *                               (ncell doubles); dJ/deps_r = -K/eps_r dJ/dK.
+ * The engine's current state afterwards is the end of the last replay. */
+int pf_adj_init(pf_engine *eng, int64_t ring_steps);
+int pf_adj_set_dft_cotangent(pf_engine *eng, int mon, const double *cot);
+int pf_adj_add_field_source(pf_engine *eng, int64_t step, int comp, const int32_t start[3],
+                            const int32_t stop[3], const int32_t stride[3],
+                            const double *vals);
+int pf_adj_segment(pf_engine *eng, int64_t step0, int64_t n, const void *state,
+                   int64_t bytes, int state_on_device);
+int pf_adj_read_grad(pf_engine *eng, double *dst);
+
 /* Steps advanced so far. */
 int pf_step(const pf_engine *eng, int64_t *step);
 

@@ -59,6 +59,11 @@ SIGNATURES = {
     "pf_read_dft": (C.c_int, [_vp, C.c_int, C.c_int, _pdbl]),
     "pf_read_flux": (C.c_int, [_vp, C.c_int, _pdbl]),
     "pf_step": (C.c_int, [_vp, _pi64]),
+    "pf_adj_init": (C.c_int, [_vp, _i64]),
+    "pf_adj_set_dft_cotangent": (C.c_int, [_vp, C.c_int, _pdbl]),
+    "pf_adj_add_field_source": (C.c_int, [_vp, _i64, C.c_int, _pi32, _pi32, _pi32, _pdbl]),
+    "pf_adj_segment": (C.c_int, [_vp, _i64, _i64, _vp, _i64, C.c_int]),
+    "pf_adj_read_grad": (C.c_int, [_vp, _pdbl]),
     "pf_write_field": (C.c_int, [_vp, C.c_int, _vp]),
     "pf_set_check_every": (C.c_int, [_vp, _i64]),
     "pf_set_wait_test": (C.c_int, [_vp, C.c_int]),

@@ -29,9 +29,14 @@ constexpr int kWarps = 8;     // warps per block
 #ifndef PFB_MINB_ASTEP
 #define PFB_MINB_ASTEP 4
 #endif
-// Minimum resident 128-thread blocks per SM of the marching forward step.
+// Minimum resident 128-thread blocks per SM of the marching forward and
+// reverse steps (forward at 12: 40 registers, measured 5% faster than at 10;
+// the reverse step needs 46-48 registers and slows down at 12).
 #ifndef PFB_MINB_MARCH
-#define PFB_MINB_MARCH 10
+#define PFB_MINB_MARCH 12
+#endif
+#ifndef PFB_MINB_AMARCH
+#define PFB_MINB_AMARCH 10
 #endif
 constexpr int kDftRing = 32;  // line samples kept before a DFT flush
 
@@ -240,8 +245,8 @@ __device__ __forceinline__ T hz_value(const BArgs<T>& a, const Inst& I, int i, i
                                       T exp_, T ex, const T* pzx, T* pzxo, const T* pzy,
                                       T* pzyo) {
   const T mch = -a.ch;
-  const T dA = qdiv(sub_rn(eyp, ey), a.dx, a.rdx, a.fdx);
-  const T dB = qdiv(sub_rn(exp_, ex), a.dy, a.rdy, a.fdy);
+  T dA, dB;
+  qdiv2(sub_rn(eyp, ey), a.dx, a.rdx, a.fdx, sub_rn(exp_, ex), a.dy, a.rdy, a.fdy, dA, dB);
   T h = add_rn(hz, mul_rn(sub_rn(dA, dB), mch));
   if (mx >= 0) {
     const long long q = I.p_hzx + (long long)mx * ny + j;
@@ -494,11 +499,13 @@ __global__ void __launch_bounds__(32 * kMarchWarps, PFB_MINB_MARCH) kb_march(
     const T hl = __shfl_up_sync(full, h, 1);  // Hz^{n+1/2} of column j - 1
     if (body && own) {
       Hzo[id] = h;
-      // Ex, Ey of (r, j): kb_e's arithmetic
+      // Ex, Ey of (r, j): kb_e's arithmetic (both quotients formed; each is
+      // used only where its difference exists)
       T cx = T(0), cy = T(0);
       T e = ex;
+      T dA, dBq;
+      qdiv2(sub_rn(h, hl), a.dy, a.rdy, a.fdy, sub_rn(h, hz_prev), a.dx, a.rdx, a.fdx, dA, dBq);
       if (j >= 1) {
-        const T dA = qdiv(sub_rn(h, hl), a.dy, a.rdy, a.fdy);
         e = add_rn(ex, mul_rn(dA, K));
         cx = dA;
         if (mye >= 0) {
@@ -513,7 +520,7 @@ __global__ void __launch_bounds__(32 * kMarchWarps, PFB_MINB_MARCH) kb_march(
       Exo[id] = e;
       e = ey;
       if (r >= 1) {
-        const T dB = qdiv(sub_rn(h, hz_prev), a.dx, a.rdx, a.fdx);
+        const T dB = dBq;
         e = add_rn(ey, mul_rn(-dB, K));
         cy = -dB;
         const int mx = a.mex[I.ox + r];
@@ -1027,7 +1034,7 @@ __global__ void __launch_bounds__(32 * kWarps, PFB_MINB_ASTEP) kb_adj_step(
 // segment that starts below row 0 first recomputes hA of row i0 - 1. Same
 // levels and arithmetic as kb_adj_step, so the same bits.
 template <typename T, bool HT, bool ET>
-__global__ void __launch_bounds__(32 * kMarchWarps, PFB_MINB_MARCH) kb_adj_march(
+__global__ void __launch_bounds__(32 * kMarchWarps, PFB_MINB_AMARCH) kb_adj_march(
     const __grid_constant__ BArgs<T> a, const __grid_constant__ AArgs<T> d, int step_t) {
   const int w = blockIdx.x * kMarchWarps + threadIdx.y;
   if (w >= a.nsegs) return;  // uniform over the warp

@@ -48,11 +48,27 @@ __device__ __forceinline__ float qdiv(float a, float d, float r, bool fast) {
 }
 __device__ __forceinline__ double qdiv_fast(double a, double d, double) { return __ddiv_rn(a, d); }
 __device__ __forceinline__ double qdiv(double a, double d, double, bool) { return __ddiv_rn(a, d); }
+// Two exact quotients sharing one range check and one branch: both by the
+// reciprocal path when it applies to both, else each by qdiv.
+template <typename T>
+__device__ __forceinline__ void qdiv2(T a0, T d0, T r0, bool f0, T a1, T d1, T r1, bool f1,
+                                      T& q0, T& q1);
 // Whether every numerator of a cell may take qdiv_fast.
 __device__ __forceinline__ bool qdiv_ok(float m) { return m < kQdivLimit; }
 __device__ __forceinline__ bool qdiv_ok(double) { return false; }
 __device__ __forceinline__ float absmax(float a, float b) { return fmaxf(fabsf(a), fabsf(b)); }
 __device__ __forceinline__ double absmax(double a, double b) { return fmax(fabs(a), fabs(b)); }
+template <typename T>
+__device__ __forceinline__ void qdiv2(T a0, T d0, T r0, bool f0, T a1, T d1, T r1, bool f1,
+                                      T& q0, T& q1) {
+  if (f0 && f1 && qdiv_ok(absmax(a0, a1))) {
+    q0 = qdiv_fast(a0, d0, r0);
+    q1 = qdiv_fast(a1, d1, r1);
+  } else {
+    q0 = qdiv(a0, d0, r0, f0);
+    q1 = qdiv(a1, d1, r1, f1);
+  }
+}
 
 // Round a double to the field type (round to nearest even).
 __device__ __forceinline__ float to_real(double v, float) { return __double2float_rn(v); }
@@ -87,6 +103,31 @@ struct MediumT {
 };
 constexpr int kMediumShift = 27;
 constexpr uint32_t kLocMask = (1u << kMediumShift) - 1u;
+
+// Soft sources of one family (simulation.py:1367-1390). Sources sharing a
+// (component, cell) form one group, applied in the reference's list order.
+struct SourceGroups {
+  const long long* cell;   // flat cell index per group
+  const int* comp;         // 0..2 within the family (x, y, z)
+  const int* start;        // group g owns sources [start[g], start[g+1])
+  const int* wave_row;     // per source
+  const double* amp;       // per source
+  const double* wave;      // [row][n_steps]
+  long long n_steps;
+  int n_groups;
+};
+
+// A DFT monitor's region: start / stride / count per axis, the components.
+struct DftRegion {
+  int start[3], stride[3], count[3];
+  long long ncell;
+  int ncomp;
+  int comps[6];
+};
+
+// Source groups and DFT monitors the split E pass handles itself.
+constexpr int kInlineSrc = 8;
+constexpr int kInlineDft = 4;
 
 // Arguments of one H + E step (split or fused kernels).
 template <typename T>
@@ -128,6 +169,33 @@ struct StepArgs {
   long long plev;  // reals per polarisation level
   int lvl;         // polarisation level holding P^n (n & 1)
   int wait_test;   // test hook of the TMA-staged step (pf_set_wait_test)
+};
+
+// Arguments of the split E pass's epilogue (the opt-in in-kernel sources
+// and DFT sampling): the E-family soft sources of this step (group g at
+// block isrc_blk[g], thread isrc_tid[g]) and the samples of the DFT monitors
+// sampled at this step (ring slot idft_slot[m], -1: none). A separate kernel
+// parameter, so the plain E pass does not carry it.
+template <typename T>
+struct EpiArgs {
+  long long step;
+  int n_isrc;
+  int isrc_blk[kInlineSrc], isrc_tid[kInlineSrc];
+  SourceGroups isrc;
+  int n_idft;
+  DftRegion idft[kInlineDft];
+  T* idft_ring[kInlineDft];
+  int idft_slot[kInlineDft];
+};
+// The epilogue parameter of k_e_split<..., EPI>: EpiArgs, or nothing.
+struct NoEpi {};
+template <typename T, bool EPI>
+struct EpiParam {
+  using type = EpiArgs<T>;
+};
+template <typename T>
+struct EpiParam<T, false> {
+  using type = NoEpi;
 };
 
 enum CeMode { kCeCell1 = 0, kCeCell3 = 1, kCeTable = 2 };

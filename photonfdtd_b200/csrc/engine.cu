@@ -22,6 +22,7 @@
 
 #include "../../include/pfb200.h"
 #include "common.cuh"
+#include "kernels_adj.cuh"
 #include "kernels_aux.cuh"
 #include "kernels_fused.cuh"
 #include "kernels_split.cuh"
@@ -130,9 +131,39 @@ struct pf_engine {
   TmaMaps maps;
   int* tma_err = nullptr;
   int wait_test = 0;     // pf_set_wait_test: one TMA stage wait runs out
+  // With env PFB200_INLINE=1 the split E pass adds the E-family sources and
+  // writes the DFT samples itself (at most kInlineSrc groups, kInlineDft
+  // monitors). Off by default: on config 3 (384^3) the epilogue instantiation
+  // of the E pass runs 0.08 ms slower per step than the plain one, more than
+  // the 0.024 ms of injection and sampling launches it replaces.
+  bool inline_epi = false;
+  int isrc_blk[kInlineSrc] = {}, isrc_tid[kInlineSrc] = {};
   long long check_every = 0;  // pf_set_check_every: non-finite scan period
   int fused_ty = 8;      // fused tile height (8 or 16), env PFB200_FUSED_TY
   int fused_chunks = 0;  // x chunks per column (0 = auto), env PFB200_XCHUNKS
+
+  // adjoint (pf_adj_*): adjoint fields, quotient and psi adjoints, the
+  // gradient, and the ring of per-step forward records a replay writes
+  bool adj = false;
+  bool recording = false;
+  long long rec_step0 = 0, ring_steps = 0, adj_next = 0;
+  void* lamE[3] = {};
+  void* lamH[3] = {};
+  void* gE[6] = {};
+  void* gH[6] = {};
+  void* lpE[6] = {};
+  void* lpH[6] = {};
+  double* grad = nullptr;
+  char* rec = nullptr;
+  size_t rec_slot = 0;          // bytes per recorded step: H (3 fields) + psi_E
+  std::vector<double*> dft_cot;  // per DFT monitor: dJ/d acc on the device, or null
+  struct RegionSource {
+    long long step;
+    int comp;
+    DftRegion r;
+    double* vals;
+  };
+  std::vector<RegionSource> rsrc;  // FieldMonitor-frame sources of the loss
 
   // launch accounting (pf_read_profile)
   long long launches[4] = {};
@@ -524,21 +555,28 @@ void launch_h_split(pf_engine* e, const StepArgs<T>& a, dim3 g, dim3 b) {
   k_h_split<T><<<g, b, 0, e->stream>>>(a);
 }
 
-template <typename T>
-void launch_e_split(pf_engine* e, const StepArgs<T>& a, dim3 g, dim3 b) {
+template <typename T, bool EPI>
+void launch_e_split_epi(pf_engine* e, const StepArgs<T>& a,
+                        const typename EpiParam<T, EPI>::type& ep, dim3 g, dim3 b) {
   const bool ade = e->n_media > 0;
   switch (e->ce_mode) {
     case PF_CE_CELL1:
-      if (ade) k_e_split<T, kCeCell1, true><<<g, b, 0, e->stream>>>(a);
-      else k_e_split<T, kCeCell1, false><<<g, b, 0, e->stream>>>(a);
+      if (ade) k_e_split<T, kCeCell1, true, EPI><<<g, b, 0, e->stream>>>(a, ep);
+      else k_e_split<T, kCeCell1, false, EPI><<<g, b, 0, e->stream>>>(a, ep);
       break;
     case PF_CE_CELL3:
-      k_e_split<T, kCeCell3, false><<<g, b, 0, e->stream>>>(a);
+      k_e_split<T, kCeCell3, false, EPI><<<g, b, 0, e->stream>>>(a, ep);
       break;
     default:
-      if (ade) k_e_split<T, kCeTable, true><<<g, b, 0, e->stream>>>(a);
-      else k_e_split<T, kCeTable, false><<<g, b, 0, e->stream>>>(a);
+      if (ade) k_e_split<T, kCeTable, true, EPI><<<g, b, 0, e->stream>>>(a, ep);
+      else k_e_split<T, kCeTable, false, EPI><<<g, b, 0, e->stream>>>(a, ep);
   }
+}
+
+template <typename T>
+void launch_e_split(pf_engine* e, const StepArgs<T>& a, const EpiArgs<T>& ep, dim3 g, dim3 b) {
+  if (e->inline_epi) launch_e_split_epi<T, true>(e, a, ep, g, b);
+  else launch_e_split_epi<T, false>(e, a, NoEpi{}, g, b);
 }
 
 template <typename T>
@@ -575,10 +613,11 @@ int flush_monitors(pf_engine* e) {
 
 // Monitors of step s read the level just written (E at t_e, H at t_h).
 template <typename T>
-int sample_monitors(pf_engine* e, long long s, int lvl) {
+int sample_monitors(pf_engine* e, long long s, int lvl, bool dft = true) {
   if (e->dfts.empty() && e->fluxes.empty()) return PF_OK;
   const Fields6<T> f = level_fields<T>(e, lvl);
   for (DftMon& m : e->dfts) {
+    if (!dft) break;  // the E pass sampled them
     if (s % m.interval) continue;
     if (m.pending == m.ring_cap) {
       int rc = flush_monitors<T>(e);
@@ -627,6 +666,25 @@ int inject(pf_engine* e, int fam, int lvl, long long s) {
   return PF_OK;
 }
 
+// An adjoint replay keeps, per step, H^{n+1/2} and psi_E after the step:
+// what the reverse step needs to recompute the gradient's g = curl + psi.
+template <typename T>
+int record_step(pf_engine* e, long long t) {
+  if (t < 0 || t >= e->ring_steps) return fail(e, PF_ERR_STATE, "record slot out of range");
+  char* base = e->rec + (size_t)t * e->rec_slot;
+  const size_t S = sizeof(T), n = (size_t)e->ncell * S;
+  size_t off = 0;
+  for (int c = 0; c < 3; ++c, off += n)
+    PF_CUDA(e, cudaMemcpyAsync(base + off, e->H[e->cur][c], n, cudaMemcpyDeviceToDevice,
+                               e->stream));
+  for (int q = 0; q < 6; ++q) {
+    const size_t b = (size_t)e->npsiE[q] * S;
+    if (b) PF_CUDA(e, cudaMemcpyAsync(base + off, e->psiE[q], b, cudaMemcpyDeviceToDevice, e->stream));
+    off += b;
+  }
+  return PF_OK;
+}
+
 template <typename T>
 int advance_typed(pf_engine* e, long long n_sub) {
   const int nz = e->nz, ny = e->ny, nx = e->nx;
@@ -661,16 +719,52 @@ int advance_typed(pf_engine* e, long long n_sub) {
       a.Hin[0] = a.Hout[0];
       a.Hin[1] = a.Hout[1];
       a.Hin[2] = a.Hout[2];
+      EpiArgs<T> ep;
+      memset(&ep, 0, sizeof ep);
+      if (e->inline_epi) {
+        ep.step = s;
+        ep.n_isrc = (int)e->src[0].cell.size();
+        for (int g = 0; g < ep.n_isrc; ++g) {
+          ep.isrc_blk[g] = e->isrc_blk[g];
+          ep.isrc_tid[g] = e->isrc_tid[g];
+        }
+        ep.isrc = e->src[0].dev;
+        // an adjoint replay (recording) samples no monitor
+        ep.n_idft = e->recording ? 0 : (int)e->dfts.size();
+        // a full ring flushes every monitor, so flush before handing out slots
+        for (const DftMon& dm : e->dfts) {
+          if (!ep.n_idft) break;
+          if (s % dm.interval == 0 && dm.pending == dm.ring_cap) {
+            const int frc = flush_monitors<T>(e);
+            if (frc) return frc;
+            break;
+          }
+        }
+        for (int m = 0; m < ep.n_idft; ++m) {
+          DftMon& dm = e->dfts[m];
+          ep.idft_slot[m] = -1;
+          if (s % dm.interval) continue;
+          ep.idft[m] = dm.r;
+          ep.idft_ring[m] = (T*)dm.ring;
+          ep.idft_slot[m] = dm.pending;
+        }
+      }
       {
         LaunchScope ls(e, 0);
-        launch_e_split<T>(e, a, grd, blk);
+        launch_e_split<T>(e, a, ep, grd, blk);
       }
-      inject<T>(e, 0, nxt, s);
+      if (e->inline_epi) {
+        for (int m = 0; m < ep.n_idft; ++m)
+          if (ep.idft_slot[m] >= 0) e->dfts[m].pending++;
+      } else {
+        inject<T>(e, 0, nxt, s);
+      }
     }
-    int rc = sample_monitors<T>(e, s, nxt);
+    int rc = e->recording ? PF_OK : sample_monitors<T>(e, s, nxt, !(e->inline_epi && !e->fused));
     if (rc) return rc;
     e->cur = nxt;
     e->step++;
+    if (e->recording && (rc = record_step<T>(e, s - e->rec_step0))) return rc;
     if (e->check_every > 0 && e->step % e->check_every == 0) {
       PF_CUDA(e, cudaGetLastError());
       if ((rc = scan_finite(e))) {
@@ -971,6 +1065,20 @@ int pf_finalize(pf_engine* e) {
   }
   int rc = e->rb == 4 ? finalize_typed<float>(e) : finalize_typed<double>(e);
   if (rc) return rc;
+  e->inline_epi = !e->fused && getenv("PFB200_INLINE") &&
+                  e->src[0].cell.size() <= (size_t)kInlineSrc &&
+                  e->dfts.size() <= (size_t)kInlineDft;
+  if (e->inline_epi) {
+    // each E source group's block and thread in the E pass's grid
+    const int bx = e->nz > 1 ? 32 : 1, by = e->nz > 1 ? 8 : 256;
+    const long long gx = (e->nz + bx - 1) / bx, gy = (e->ny + by - 1) / by;
+    for (size_t g = 0; g < e->src[0].cell.size(); ++g) {
+      const long long c = e->src[0].cell[g];
+      const long long i = c / ((long long)e->ny * e->nz), j = (c / e->nz) % e->ny, k = c % e->nz;
+      e->isrc_blk[g] = (int)((i * gy + j / by) * gx + k / bx);
+      e->isrc_tid[g] = (int)((j % by) * bx + k % bx);
+    }
+  }
   // host staging no longer needed
   for (int c = 0; c < 3; ++c) std::vector<char>().swap(e->h_ce[c]);
   std::vector<uint32_t>().swap(e->h_word);
@@ -1246,6 +1354,231 @@ void pf_destroy(pf_engine* e) {
   for (cudaEvent_t ev : e->ev_pool) cudaEventDestroy(ev);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Adjoint of the stepping (value_and_grad_eps, jaxbackend.py:666-722): the
+// caller checkpoints the forward run with pf_get_state, hands the loss's
+// sensitivities to its outputs to pf_adj_set_dft_cotangent /
+// pf_adj_add_field_source, then calls pf_adj_segment on the checkpointed
+// segments from the last to the first. Each call restores the segment's
+// state, replays it recording H^{n+1/2} and psi_E per step (no monitor
+// sampling), and runs its reverse steps (kernels_adj.cuh), accumulating
+// dJ/dK per cell.
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename T>
+AdjState<T> adj_state(pf_engine* e, long long slot) {
+  AdjState<T> s;
+  memset(&s, 0, sizeof s);
+  const char* base = e->rec + (size_t)slot * e->rec_slot;
+  const size_t S = sizeof(T), n = (size_t)e->ncell * S;
+  size_t off = 0;
+  for (int c = 0; c < 3; ++c, off += n) s.Hrec[c] = (const T*)(base + off);
+  for (int q = 0; q < 6; ++q) {
+    s.psiErec[q] = (const T*)(base + off);
+    off += (size_t)e->npsiE[q] * S;
+  }
+  for (int c = 0; c < 3; ++c) {
+    s.lamE[c] = (T*)e->lamE[c];
+    s.lamH[c] = (T*)e->lamH[c];
+  }
+  for (int q = 0; q < 6; ++q) {
+    s.gE[q] = (T*)e->gE[q];
+    s.gH[q] = (T*)e->gH[q];
+    s.lpE[q] = (T*)e->lpE[q];
+    s.lpH[q] = (T*)e->lpH[q];
+  }
+  s.grad = e->grad;
+  for (int a = 0; a < 3; ++a) s.idl[a] = (T)(1.0 / e->dl[a]);
+  return s;
+}
+
+// The loss's sources on the fields sampled at step m, family fam (0: E^{m+1},
+// 1: H^{m+1/2}).
+template <typename T>
+int adj_sources(pf_engine* e, long long m, int fam) {
+  const int B = 256;
+  T* l[3];
+  for (int c = 0; c < 3; ++c) l[c] = (T*)(fam == 0 ? e->lamE[c] : e->lamH[c]);
+  for (size_t k = 0; k < e->dfts.size(); ++k) {
+    const DftMon& dm = e->dfts[k];
+    if (!e->dft_cot[k] || m % dm.interval) continue;
+    const long long q = m / dm.interval;
+    const double* ph = (fam == 0 ? dm.ph_e : dm.ph_h) + q * dm.n_freq * 2;
+    const long long nt = dm.r.ncell * dm.r.ncomp;
+    k_adj_dft_src<T><<<(unsigned)((nt + B - 1) / B), B, 0, e->stream>>>(
+        dm.r, e->dft_cot[k], ph, dm.n_freq, dm.dt, fam, l[0], l[1], l[2], e->ny, e->nz);
+  }
+  for (const auto& rs : e->rsrc) {
+    if (rs.step != m || (rs.comp >= 3) != (fam == 1)) continue;
+    k_adj_region_src<T><<<(unsigned)((rs.r.ncell + B - 1) / B), B, 0, e->stream>>>(
+        rs.r, rs.vals, l[rs.comp % 3], e->ny, e->nz);
+  }
+  PF_CUDA(e, cudaGetLastError());
+  return PF_OK;
+}
+
+template <typename T>
+int adj_segment_typed(pf_engine* e, long long step0, long long n) {
+  e->recording = true;
+  e->rec_step0 = step0;
+  int rc = advance_typed<T>(e, n);
+  e->recording = false;
+  if (rc) return rc;
+  const int nz = e->nz, ny = e->ny, nx = e->nx;
+  const dim3 blk = nz > 1 ? dim3(32, 8) : dim3(1, 256);
+  const dim3 grd((nz + blk.x - 1) / blk.x, (ny + blk.y - 1) / blk.y, nx);
+  const StepArgs<T> a = step_args<T>(e);
+  for (long long m = step0 + n - 1; m >= step0; --m) {
+    const AdjState<T> s = adj_state<T>(e, m - step0);
+    if ((rc = adj_sources<T>(e, m, 0))) return rc;
+    if (e->ce_mode == PF_CE_CELL1)
+      k_adj_e<T, kCeCell1><<<grd, blk, 0, e->stream>>>(a, s);
+    else
+      k_adj_e<T, kCeTable><<<grd, blk, 0, e->stream>>>(a, s);
+    if ((rc = adj_sources<T>(e, m, 1))) return rc;
+    k_adj_h<T><<<grd, blk, 0, e->stream>>>(a, s);
+  }
+  PF_CUDA(e, cudaGetLastError());
+  PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  e->adj_next = step0;
+  return PF_OK;
+}
+
+int adj_zero(pf_engine* e) {
+  const size_t S = e->rb, n = (size_t)e->ncell * S;
+  for (int c = 0; c < 3; ++c) {
+    PF_CUDA(e, cudaMemsetAsync(e->lamE[c], 0, n, e->stream));
+    PF_CUDA(e, cudaMemsetAsync(e->lamH[c], 0, n, e->stream));
+  }
+  for (int q = 0; q < 6; ++q) {
+    PF_CUDA(e, cudaMemsetAsync(e->gE[q], 0, n, e->stream));
+    PF_CUDA(e, cudaMemsetAsync(e->gH[q], 0, n, e->stream));
+    if (e->npsiE[q]) PF_CUDA(e, cudaMemsetAsync(e->lpE[q], 0, e->npsiE[q] * S, e->stream));
+    if (e->npsiH[q]) PF_CUDA(e, cudaMemsetAsync(e->lpH[q], 0, e->npsiH[q] * S, e->stream));
+  }
+  PF_CUDA(e, cudaMemsetAsync(e->grad, 0, (size_t)e->ncell * 8, e->stream));
+  PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  e->adj_next = e->n_steps;
+  return PF_OK;
+}
+
+bool make_region(pf_engine* e, const int32_t start[3], const int32_t stop[3],
+                 const int32_t stride[3], DftRegion& r) {
+  const int dims[3] = {e->nx, e->ny, e->nz};
+  r.ncell = 1;
+  r.ncomp = 1;
+  for (int a = 0; a < 3; ++a) {
+    if (start[a] < 0 || stop[a] > dims[a] || stop[a] <= start[a] || stride[a] < 1) return false;
+    r.start[a] = start[a];
+    r.stride[a] = stride[a];
+    r.count[a] = (stop[a] - start[a] + stride[a] - 1) / stride[a];
+    r.ncell *= r.count[a];
+  }
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pf_adj_init(pf_engine* e, int64_t ring_steps) {
+  if (!e) return PF_ERR_INVALID;
+  if (!e->finalized) return fail(e, PF_ERR_STATE, "pf_adj_init before pf_finalize");
+  if (e->n_media > 0)
+    return fail(e, PF_ERR_UNSUPPORTED, "the adjoint does not cover dispersive (ADE) media");
+  if (e->ce_mode == PF_CE_CELL3)
+    return fail(e, PF_ERR_UNSUPPORTED,
+                "the adjoint differentiates one coefficient per cell, not a subpixel tensor");
+  if (ring_steps < 1 || ring_steps > e->n_steps)
+    return fail(e, PF_ERR_INVALID, "ring_steps %lld outside [1, n_steps]", (long long)ring_steps);
+  PF_CUDA(e, cudaSetDevice(e->device));
+  int rc;
+  const size_t S = e->rb, n = (size_t)e->ncell * S;
+  if (!e->adj) {
+    for (int c = 0; c < 3; ++c) {
+      if ((rc = dalloc(e, &e->lamE[c], n))) return rc;
+      if ((rc = dalloc(e, &e->lamH[c], n))) return rc;
+    }
+    for (int q = 0; q < 6; ++q) {
+      if ((rc = dalloc(e, &e->gE[q], n))) return rc;
+      if ((rc = dalloc(e, &e->gH[q], n))) return rc;
+      if ((rc = dalloc(e, &e->lpE[q], e->npsiE[q] * S))) return rc;
+      if ((rc = dalloc(e, &e->lpH[q], e->npsiH[q] * S))) return rc;
+    }
+    if ((rc = dalloc(e, (void**)&e->grad, (size_t)e->ncell * 8))) return rc;
+    e->dft_cot.assign(e->dfts.size(), nullptr);
+    e->adj = true;
+  }
+  if (ring_steps > e->ring_steps) {
+    size_t slot = 3 * n;
+    for (int q = 0; q < 6; ++q) slot += e->npsiE[q] * S;
+    e->rec_slot = (slot + 255) & ~(size_t)255;
+    // the old ring stays allocated (freed with the engine)
+    if ((rc = dalloc(e, (void**)&e->rec, e->rec_slot * (size_t)ring_steps))) return rc;
+    e->ring_steps = ring_steps;
+  }
+  return adj_zero(e);
+}
+
+int pf_adj_set_dft_cotangent(pf_engine* e, int mon, const double* cot) {
+  if (!e || !cot) return PF_ERR_INVALID;
+  if (!e->adj) return fail(e, PF_ERR_STATE, "pf_adj_set_dft_cotangent before pf_adj_init");
+  if (mon < 0 || mon >= (int)e->dfts.size()) return fail(e, PF_ERR_INVALID, "bad DFT monitor");
+  const DftMon& dm = e->dfts[mon];
+  const size_t bytes = (size_t)dm.r.ncomp * dm.n_freq * dm.r.ncell * 16;
+  int rc;
+  if (!e->dft_cot[mon] && (rc = dalloc(e, (void**)&e->dft_cot[mon], bytes))) return rc;
+  PF_CUDA(e, cudaMemcpyAsync(e->dft_cot[mon], cot, bytes, cudaMemcpyHostToDevice, e->stream));
+  PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  return PF_OK;
+}
+
+int pf_adj_add_field_source(pf_engine* e, int64_t step, int comp, const int32_t start[3],
+                            const int32_t stop[3], const int32_t stride[3], const double* vals) {
+  if (!e || !vals || !start || !stop || !stride) return PF_ERR_INVALID;
+  if (!e->adj) return fail(e, PF_ERR_STATE, "pf_adj_add_field_source before pf_adj_init");
+  if (!valid_comp(comp) || step < 0 || step >= e->n_steps)
+    return fail(e, PF_ERR_INVALID, "bad component or step");
+  pf_engine::RegionSource rs;
+  rs.step = step;
+  rs.comp = comp;
+  if (!make_region(e, start, stop, stride, rs.r)) return fail(e, PF_ERR_INVALID, "bad region");
+  int rc;
+  if ((rc = dalloc(e, (void**)&rs.vals, (size_t)rs.r.ncell * 8))) return rc;
+  PF_CUDA(e, cudaMemcpyAsync(rs.vals, vals, (size_t)rs.r.ncell * 8, cudaMemcpyHostToDevice,
+                             e->stream));
+  PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  e->rsrc.push_back(rs);
+  return PF_OK;
+}
+
+int pf_adj_segment(pf_engine* e, int64_t step0, int64_t n, const void* state, int64_t bytes,
+                   int state_on_device) {
+  if (!e || !state) return PF_ERR_INVALID;
+  if (!e->adj) return fail(e, PF_ERR_STATE, "pf_adj_segment before pf_adj_init");
+  if (n < 1 || n > e->ring_steps || step0 < 0 || step0 + n != e->adj_next)
+    return fail(e, PF_ERR_STATE,
+                "segment [%lld, %lld) must end where the reverse pass stands (%lld) and hold at "
+                "most %lld steps",
+                (long long)step0, (long long)(step0 + n), e->adj_next, e->ring_steps);
+  int rc = e->rb == 4 ? flush_monitors<float>(e) : flush_monitors<double>(e);
+  if (rc) return rc;
+  if ((rc = copy_state(e, step0, const_cast<void*>(state), bytes, state_on_device, false)))
+    return rc;
+  e->step = step0;
+  return e->rb == 4 ? adj_segment_typed<float>(e, step0, n) : adj_segment_typed<double>(e, step0, n);
+}
+
+int pf_adj_read_grad(pf_engine* e, double* dst) {
+  if (!e || !dst) return PF_ERR_INVALID;
+  if (!e->adj) return fail(e, PF_ERR_STATE, "pf_adj_read_grad before pf_adj_init");
+  PF_CUDA(e, cudaMemcpy(dst, e->grad, (size_t)e->ncell * 8, cudaMemcpyDeviceToHost));
+  return PF_OK;
 }
 
 }  // extern "C"

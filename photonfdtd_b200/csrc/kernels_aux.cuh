@@ -11,17 +11,6 @@ namespace pfb {
 // each as a double add rounded to the field type, so coincident dipoles round
 // exactly as the reference's successive `F[i,j,k] += val` do.
 // ---------------------------------------------------------------------------
-struct SourceGroups {
-  const long long* cell;   // flat cell index per group
-  const int* comp;         // 0..2 within the family (x, y, z)
-  const int* start;        // group g owns sources [start[g], start[g+1])
-  const int* wave_row;     // per source
-  const double* amp;       // per source
-  const double* wave;      // [row][n_steps]
-  long long n_steps;
-  int n_groups;
-};
-
 template <typename T>
 __global__ void k_inject(SourceGroups s, T* f0, T* f1, T* f2, long long step) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -47,13 +36,6 @@ __global__ void k_inject(SourceGroups s, T* f0, T* f1, T* f2, long long step) {
 template <typename T>
 struct Fields6 {
   const T* f[6];
-};
-
-struct DftRegion {
-  int start[3], stride[3], count[3];
-  long long ncell;
-  int ncomp;
-  int comps[6];
 };
 
 template <typename T>

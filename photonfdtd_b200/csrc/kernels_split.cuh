@@ -121,15 +121,98 @@ __global__ void __launch_bounds__(256, PFB_MINB_H) k_h_split(const __grid_consta
   h_cell<T>(a, i, j, k, box);
 }
 
-// E pass: E^{n+1} = E^n + ce (curl H^{n+1/2} + psi), then ADE.
-template <typename T, int CE, bool ADE>
-__global__ void __launch_bounds__(256, PFB_MINB_E) k_e_split(const __grid_constant__ StepArgs<T> a) {
+// The E pass's epilogue, after the curl and ADE updates of cell (i, j, k):
+// the E-family soft sources of the cell, each group's sources added in list
+// order in double and rounded once (k_inject's arithmetic), then the cell's
+// samples for the DFT monitors sampled this step (E after the sources, H
+// at n + 1/2: the values k_dft_sample reads after the step).
+template <typename T>
+__device__ __forceinline__ void e_epilogue(const StepArgs<T>& a, const EpiArgs<T>& ep, int i,
+                                           int j, int k, long long id, T e[3]) {
+  if (ep.n_isrc) {
+    const int blk = (int)((blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
+    const int tid = (int)(threadIdx.y * blockDim.x + threadIdx.x);
+    for (int g = 0; g < ep.n_isrc; ++g) {
+      if (blk != ep.isrc_blk[g] || tid != ep.isrc_tid[g]) continue;
+      const SourceGroups& s = ep.isrc;
+      const int c = s.comp[g];
+      T v = e[c];
+      for (int q = s.start[g]; q < s.start[g + 1]; ++q)
+        v = add_double<T>(v, __dmul_rn(s.amp[q],
+                                       s.wave[(long long)s.wave_row[q] * s.n_steps + ep.step]));
+      e[c] = v;
+    }
+  }
+  for (int m = 0; m < ep.n_idft; ++m) {
+    if (ep.idft_slot[m] < 0) continue;
+    const DftRegion& r = ep.idft[m];
+    // the bounding box first (unsigned: below start wraps high); the
+    // divisions only for cells inside it on a strided axis
+    const unsigned di = (unsigned)(i - r.start[0]), dj = (unsigned)(j - r.start[1]),
+                   dk = (unsigned)(k - r.start[2]);
+    if (di >= (unsigned)((r.count[0] - 1) * r.stride[0] + 1) ||
+        dj >= (unsigned)((r.count[1] - 1) * r.stride[1] + 1) ||
+        dk >= (unsigned)((r.count[2] - 1) * r.stride[2] + 1))
+      continue;
+    int ci = (int)di, cj = (int)dj, ck = (int)dk;
+    if (r.stride[0] > 1 || r.stride[1] > 1 || r.stride[2] > 1) {
+      if (di % r.stride[0] || dj % r.stride[1] || dk % r.stride[2]) continue;
+      ci = (int)di / r.stride[0];
+      cj = (int)dj / r.stride[1];
+      ck = (int)dk / r.stride[2];
+      if (ci >= r.count[0] || cj >= r.count[1] || ck >= r.count[2]) continue;
+    }
+    const long long cell = ((long long)ci * r.count[1] + cj) * r.count[2] + ck;
+    T* ring = ep.idft_ring[m] + (long long)ep.idft_slot[m] * r.ncomp * r.ncell;
+    for (int q = 0; q < r.ncomp; ++q) {
+      // H is reloaded here (a cache hit) rather than kept live through the
+      // update for the few cells that sample it
+      const int c = r.comps[q];
+      ring[(long long)q * r.ncell + cell] = c < 3 ? e[c] : a.Hin[c - 3][id];
+    }
+  }
+}
+
+// Whether block (blockIdx) holds a source cell of this step or cells of a
+// DFT region sampled at this step (uniform over the block), so that every
+// other block skips the epilogue after one test.
+template <typename T>
+__device__ __forceinline__ bool epilogue_block(const EpiArgs<T>& a) {
+  if (a.n_isrc) {
+    const int blk = (int)((blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x);
+    for (int g = 0; g < a.n_isrc; ++g)
+      if (blk == a.isrc_blk[g]) return true;
+  }
+  const int i = blockIdx.z;
+  const int j0 = blockIdx.y * blockDim.y, j1 = j0 + blockDim.y;
+  const int k0 = blockIdx.x * blockDim.x, k1 = k0 + blockDim.x;
+  for (int m = 0; m < a.n_idft; ++m) {
+    if (a.idft_slot[m] < 0) continue;
+    const DftRegion& r = a.idft[m];
+    const int hi0 = r.start[0] + (r.count[0] - 1) * r.stride[0] + 1;
+    const int hi1 = r.start[1] + (r.count[1] - 1) * r.stride[1] + 1;
+    const int hi2 = r.start[2] + (r.count[2] - 1) * r.stride[2] + 1;
+    if (i >= r.start[0] && i < hi0 && j1 > r.start[1] && j0 < hi1 && k1 > r.start[2] && k0 < hi2)
+      return true;
+  }
+  return false;
+}
+
+// E pass: E^{n+1} = E^n + ce (curl H^{n+1/2} + psi), then ADE; with EPI the
+// epilogue above (a separate instantiation: the plain pass carries none of
+// its code).
+template <typename T, int CE, bool ADE, bool EPI>
+__global__ void __launch_bounds__(256, PFB_MINB_E)
+    k_e_split(const __grid_constant__ StepArgs<T> a,
+              const __grid_constant__ typename EpiParam<T, EPI>::type ep) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
   const bool box = in_box(i, blockIdx.y * blockDim.y, (blockIdx.y + 1) * blockDim.y,
                           blockIdx.x * blockDim.x, (blockIdx.x + 1) * blockDim.x, a.eb0, a.eb1);
   const MediumT<T>* media = a.media;
+  bool epi = false;
+  if constexpr (EPI) epi = (ep.n_isrc || ep.n_idft) && epilogue_block<T>(ep);
   if (k >= a.nz || j >= a.ny) return;
   const long long sy = a.nz, sx = (long long)a.ny * a.nz;
   const long long id = i * sx + j * sy + k;
@@ -183,6 +266,9 @@ __global__ void __launch_bounds__(256, PFB_MINB_E) k_e_split(const __grid_consta
                      ld_if(a.Hin[0], id, -sy, ly));
   }
   if (ADE && w) ade_update<T>(a, media, rec, en, e);
+  if constexpr (EPI) {
+    if (epi) e_epilogue<T>(a, ep, i, j, k, id, e);
+  }
   a.Eout[0][id] = e[0];
   a.Eout[1][id] = e[1];
   a.Eout[2][id] = e[2];

@@ -438,6 +438,11 @@ class B200Engine:
         self._cache.clear()
         self._chk(self._L.pf_set_state(self.h, int(step), N.ptr(b), b.size, 0))
 
+    def get_state_to(self, dev_ptr: int, nbytes: int) -> None:
+        """Copy the state blob into device memory at dev_ptr (nbytes long)."""
+        import ctypes as C
+        self._chk(self._L.pf_get_state(self.h, C.c_void_p(dev_ptr), int(nbytes), 1))
+
     def step(self) -> int:
         import ctypes as C
         v = C.c_int64()
@@ -603,13 +608,12 @@ def result_bytes(res) -> int:
     return int(n + 8 * len(res.flux))
 
 
-def drive(sim, eng: B200Engine, t: dict, mon_dtype=None):
+def field_plans(sim, n_steps: int, dt: float) -> Dict[str, dict]:
+    """Per FieldMonitor: the steps after which a frame is taken and the
+    snapshot region (start, stop, stride) (simulation.py:1062-1067: one z
+    plane with plane_z, else every downsample-th cell per axis)."""
     grid = sim.grid
-    dt, n_steps = t["dt"], t["n_steps"]
-    mon_dtype = sim.dtypes["monitors"] if mon_dtype is None else mon_dtype
-    Result = _result_cls(sim)
-    result = Result(times=np.arange(n_steps) * dt)
-    rec: Dict[str, dict] = {}
+    plans: Dict[str, dict] = {}
     for m in sim.monitors:
         if type(m).__name__ != "FieldMonitor":
             continue
@@ -617,8 +621,6 @@ def drive(sim, eng: B200Engine, t: dict, mon_dtype=None):
             steps = {int(round(tt / dt)) for tt in m.times if 0 <= int(round(tt / dt)) < n_steps}
         else:
             steps = set(range(0, n_steps, m.interval))
-        # the snapshot region (simulation.py:1062-1067): one z plane with
-        # plane_z, else every downsample-th cell per axis
         ds = max(int(m.downsample), 1)
         shape = tuple(grid.shape)
         if m.plane_z is not None:
@@ -626,8 +628,21 @@ def drive(sim, eng: B200Engine, t: dict, mon_dtype=None):
             region = ((0, 0, zi), (shape[0], shape[1], zi + 1), (ds, ds, 1))
         else:
             region = ((0, 0, 0), shape, (ds, ds, ds))
-        rec[m.name] = dict(m=m, steps=steps, region=region, n=len(steps), count=0,
-                           store={c: None for c in m.components}, times=[])
+        plans[m.name] = dict(m=m, steps=steps, region=region)
+    return plans
+
+
+def drive(sim, eng: B200Engine, t: dict, mon_dtype=None):
+    grid = sim.grid
+    dt, n_steps = t["dt"], t["n_steps"]
+    mon_dtype = sim.dtypes["monitors"] if mon_dtype is None else mon_dtype
+    Result = _result_cls(sim)
+    result = Result(times=np.arange(n_steps) * dt)
+    rec: Dict[str, dict] = {}
+    for name, p in field_plans(sim, n_steps, dt).items():
+        m = p["m"]
+        rec[name] = dict(m=m, steps=p["steps"], region=p["region"], n=len(p["steps"]),
+                         count=0, store={c: None for c in m.components}, times=[])
 
     stop_steps = sorted(set().union(*(r["steps"] for r in rec.values()))) if rec else []
     cb = getattr(sim, "progress_callback", None)

@@ -60,3 +60,26 @@ def test_engine_bitwise_against_oracle(name):
     scale = max([abs(v) for v in ref["flux"].values()] + [1e-300])
     for mon, v in ref["flux"].items():
         assert abs(res.flux[mon] - v) <= 1e-6 * scale, (name, mon, res.flux[mon], v)
+
+
+@pytest.mark.parametrize("name", ["xz2d_f32", "tm2d_f64", "disp2d_f32", "sub3d_f32"])
+def test_inline_sources_and_dft_equal_separate_launches(name, monkeypatch):
+    """With PFB200_INLINE=1 the split E pass adds the E-family sources and
+    writes the DFT samples itself; by default separate kernels do it after
+    the pass. Fields, DFT sums and flux must be identical either way."""
+    out = []
+    for on in (True, False):
+        if on:
+            monkeypatch.setenv("PFB200_INLINE", "1")
+        else:
+            monkeypatch.delenv("PFB200_INLINE", raising=False)
+        out.append(scenes.build(name, pf).run())
+    a, b = out
+    for mon, comps in a.fields.items():
+        for c, arr in comps.items():
+            np.testing.assert_array_equal(arr, b.fields[mon][c], err_msg=f"{name} {mon} {c}")
+    for mon, comps in a.dft.items():
+        for c, arr in comps.items():
+            np.testing.assert_array_equal(arr, b.dft[mon][c], err_msg=f"{name} dft {mon} {c}")
+    for mon, v in a.flux.items():
+        assert v == b.flux[mon], (name, mon)
