@@ -75,6 +75,10 @@ def parse():
     p.add_argument("--no-surrogate", action="store_true",
                    help="skip the surrogate tensor-core GEMM / training-step figures")
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--no-adjoint3d", action="store_true",
+                   help="skip the single-scene 3D gradient leg")
+    p.add_argument("--only-adjoint3d", action="store_true",
+                   help="print only the single-scene 3D gradient leg")
     p.add_argument("--adjoint-iters", type=int, default=2)
     p.add_argument("--only-adjoint", action="store_true",
                    help="time the config-4 gradient iteration alone (profiling)")
@@ -582,6 +586,62 @@ def adjoint_bench(iters: int, cpu: bool, n_inst: int = 256, n_steps: int = 4000)
     return out
 
 
+def adjoint3d_bench(n: int = 192, n_steps: int = 2000) -> dict:
+    """value_and_grad_eps of one 3D scene (photonfdtd_b200.adjoint): n^3
+    cells at 20 nm with a 12-cell CPML, float32, four dielectric boxes, an Ex
+    dipole, an Ex / Ey DFT on the z = 0 plane at 4 wavelengths, J = sum |DFT|^2.
+    Times the forward run alone and the full gradient (forward with
+    checkpoints, then per segment a replay and the reverse steps), wall
+    clock around synchronised calls."""
+    import time
+    import torch
+    import photonfdtd_b200 as pf
+    from photonfdtd_b200.adjoint import value_and_grad_eps
+    from photonfdtd_b200.engine import run_b200
+    d = 20e-9
+    L = n * d
+    grid = pf.Grid(size=(L, L, L), cell_size=d, pml_layers=(12, 12, 12))
+    boxes = [pf.Box(center=(cx * L, cy * L, 0.0), size=(0.12 * L, 0.1 * L, 0.3 * L),
+                    medium=pf.Medium(permittivity=ep))
+             for cx, cy, ep in ((0.1, 0.05, 4.0), (-0.12, 0.1, 2.25), (0.05, -0.15, 6.0),
+                                (-0.05, -0.05, 3.0))]
+    f0 = 299_792_458.0 / 0.8e-6
+    src = pf.PointDipole(position=(-0.25 * L, 0.0, 0.0), component="Ex",
+                         waveform=pf.GaussianPulse(freq0=f0, fwhm=4e-15))
+    dft = pf.DFTMonitor(name="d", components=("Ex", "Ey"),
+                        freqs=list(f0 * np.array([0.9, 1.0, 1.1, 1.2])),
+                        plane_axis="z", plane_position=0.0)
+    dt = pf.Simulation(grid, structures=boxes, sources=[src], monitors=[dft],
+                       run_time=1e-15, precision="float32").dt
+    sim = pf.Simulation(grid, structures=boxes, sources=[src], monitors=[dft],
+                        run_time=(n_steps - 0.5) * dt, precision="float32")
+
+    def loss(out):
+        return sum((v.abs() ** 2).sum() for v in out["dft"]["d"].values())
+
+    run_b200(sim)  # warm-up (tables, module load)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    run_b200(sim)
+    torch.cuda.synchronize()
+    t_fwd = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    val, g = value_and_grad_eps(sim, loss)
+    torch.cuda.synchronize()
+    t_grad = time.perf_counter() - t0
+    cells = n ** 3
+    return {"workload": f"{n}^3 cells (12-cell CPML) at 20 nm, float32, 4 dielectric boxes, Ex "
+                        f"dipole, Ex/Ey DFT on z = 0 at 4 wavelengths, {int(sim.n_steps)} steps, "
+                        "J = sum |DFT|^2",
+            "cells": cells, "steps": int(sim.n_steps),
+            "checkpoint_every": int(np.ceil(np.sqrt(sim.n_steps))),
+            "forward_s": round(t_fwd, 3), "value_and_grad_s": round(t_grad, 3),
+            "grad_over_forward": round(t_grad / t_fwd, 2),
+            "reverse_mcell_steps_per_s": round(cells * sim.n_steps / max(t_grad - t_fwd, 1e-9)
+                                               / 1e6, 1),
+            "finite": bool(np.isfinite(g).all()), "value": float(val)}
+
+
 def adjoint_cpu_baseline(sim, win, cells_total, steps=60):
     """The NumPy forward + adjoint restatement (oracle/adjoint2d.py) on the
     first instance for `steps` steps, scaled by cell-steps to the batch."""
@@ -601,6 +661,9 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.only_adjoint3d:
+        print(json.dumps(adjoint3d_bench()), flush=True)
+        return
     if args.only_adjoint:
         adj = adjoint_bench(max(1, args.adjoint_iters), False, args.adjoint_instances,
                             args.adjoint_steps)
@@ -704,6 +767,8 @@ def main():
             adj["value"] = round(max_over_ranks(adj["value"], dist), 3)
             adj["scaling"] = "weak (one batch per rank)"
         line["adjoint"] = adj
+    if rank == 0 and world == 1 and not args.no_adjoint3d:
+        line["adjoint3d"] = adjoint3d_bench()
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         line["reference_gpu"] = reference_gpu_bench(args.size)
     if rank == 0 and world == 1 and not args.no_surrogate:

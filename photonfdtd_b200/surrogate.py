@@ -811,7 +811,8 @@ def surrogate_loop(problem: FDTDDesignProblem, net: SurrogateNet, param: SmoothD
                    verify_every: int = 10, max_error: float = 0.02,
                    tuner: Optional[OnlineTuner] = None, target: Optional[float] = None,
                    fallback_steps: int = 1, max_tries: int = 3, burst_lr: Optional[float] = None,
-                   max_bursts: int = 1) -> Dict:
+                   max_bursts: int = 1, grow: float = 1.0, max_burst_len: int = 80,
+                   wall_budget: Optional[float] = None) -> Dict:
     """Surrogate-assisted gradient ascent on z with first-order model
     management (the additive-correction trust-region scheme of Alexandrov,
     Dennis, Lewis and Torczon, 1998). Each cycle:
@@ -835,7 +836,11 @@ def surrogate_loop(problem: FDTDDesignProblem, net: SurrogateNet, param: SmoothD
     Every FDTD spectrum feeds `tuner` (online fine-tuning). Iterations are
     design updates: FDTD steps and kept surrogate steps count toward `iters`,
     rolled-back bursts do not. With `target`, records the wall-clock at which
-    the best verified objective first reaches target - 1 % |target|."""
+    the best verified objective first reaches target - 1 % |target|.
+    `grow` > 1 adapts the burst length: a kept burst multiplies it by grow
+    (at most max_burst_len steps), a rejected one halves it (at least 2).
+    `wall_budget` (seconds) ends the loop at the first cycle boundary past
+    it, whatever `iters` says."""
     z = np.array(z0, np.float64)
     opt = _Adam(z.shape, lr)
     blr = lr if burst_lr is None else burst_lr
@@ -855,7 +860,10 @@ def surrogate_loop(problem: FDTDDesignProblem, net: SurrogateNet, param: SmoothD
         if target is not None and reached is None and best_v >= target - 0.01 * abs(target):
             reached = time.perf_counter() - t0
 
+    burst_len = verify_every
     while it < iters:
+        if wall_budget is not None and time.perf_counter() - t0 >= wall_budget:
+            break
         # 1. plain FDTD steps; the last one's gradient corrects the surrogate
         for _ in range(min(n_plain, iters - it)):
             rho = param.rho(z)
@@ -886,7 +894,7 @@ def surrogate_loop(problem: FDTDDesignProblem, net: SurrogateNet, param: SmoothD
         while kept < max_bursts and rejected < max_tries and it < iters:
             saved = (z.copy(), opt.m.copy(), opt.v.copy(), opt.t)
             opt.lr = step
-            n = min(verify_every, iters - it)
+            n = min(burst_len, iters - it)
             for _ in range(n):
                 _, gs = net.value_and_grad(param.rho(z), band_objective)
                 z = opt.ascend(z, param.grad_z(z, gs + delta))
@@ -903,11 +911,15 @@ def surrogate_loop(problem: FDTDDesignProblem, net: SurrogateNet, param: SmoothD
                 n_kept += n
                 kept += 1
                 note(vt, z)
+                if grow > 1.0:
+                    burst_len = min(max_burst_len, int(round(burst_len * grow)))
             else:
                 z, opt.m, opt.v, opt.t = saved
                 step *= 0.5
                 rejected += 1
                 n_reject += 1
+                if grow > 1.0:
+                    burst_len = max(2, burst_len // 2)
         n_plain = fallback_steps if perr > max_error else 1
         log.append({"iter": it, "t": round(time.perf_counter() - t0, 3), "best": best_v,
                     "objective": cur_v, "bursts_kept": kept, "bursts_rejected": rejected,
