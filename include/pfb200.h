@@ -365,20 +365,19 @@ int pfb_set_dft(pf_batch *b, int n_freq, const double *phase);
  * the state is stored every K steps (ceil(n_steps/K) - 1 states), and the
  * adjoint replays K steps at a time; K >= n_steps stores no state and needs
  * no replay. K = 0 makes a forward-only batch: no adjoint state is allocated
- * and pfb_adjoint / pfb_read_grad return PF_ERR_STATE. tile_rows: x rows per 32-wide tile (4, 8, 16 or 32; a
- * thread updates tile_rows / 4 consecutive rows; the marching segments are
- * 2 x tile_rows rows high). */
+ * and pfb_adjoint / pfb_read_grad return PF_ERR_STATE. tile_rows: x rows per 32-wide tile (8, 16 or 32; a thread
+ * updates tile_rows / 8 consecutive rows). */
 int pfb_finalize(pf_batch *b, int checkpoint_every, int tile_rows);
 
-/* Re-lays the work lists at another tile height (4, 8, 16 or 32 x rows) after
- * pfb_finalize; allocates nothing (the buffers are sized for 4). Results
+/* Re-lays the work list at another tile height (8, 16 or 32 x rows) after
+ * pfb_finalize; allocates nothing (the tile buffer is sized for 8). Results
  * do not depend on the tile height. No counterpart in the reference (its
  * GPU path launches one thread per cell, rust/src/cuda.rs:298-341). */
 int pfb_set_tile_rows(pf_batch *b, int tile_rows);
-/* The tile-height autotuner: for 4, 8, 16 and 32 rows, runs trial_steps
- * forward steps (clamped to the checkpoint spacing and n_steps) once to
- * capture their graph and once timed by CUDA events on the batch stream;
- * writes the four ms per step to ms_per_step[4], keeps the fastest height (*best_rows)
+/* The tile-height autotuner: for 8, 16 and 32 rows, runs trial_steps forward
+ * steps (clamped to the checkpoint spacing and n_steps) once to capture
+ * their graph and once timed by CUDA events on the batch stream; writes the
+ * three ms per step to ms_per_step[3], keeps the fastest height (*best_rows)
  * and resets the state (fields, ring, DFT sums): call it before pfb_forward.
  * No counterpart in the reference. */
 int pfb_tune_tiles(pf_batch *b, int trial_steps, float *ms_per_step, int *best_rows);
@@ -404,11 +403,9 @@ int pfb_read_grad(pf_batch *b, double *dst);
 /* Component comp (0 Ex, 1 Ey, 2 Hz) of instance k, nx*ny reals. */
 int pfb_read_field(pf_batch *b, int k, int comp, void *dst);
 /* out[0..n_out): cells, line cells, design cells, tiles, K, segments,
- * reals per stored state, kernel launches issued so far, 1 when the forward
- * and reverse steps run as one fused launch each on double-buffered state
- * (every batch without Hz sources) and 0 for the split passes, then the
- * marching segments and how many of them are bulk segments (no face, CPML
- * or design cell within reach; stepped by their own leaner kernels). */
+ * reals per stored state, kernel launches issued so far, and 1 when the
+ * forward and reverse steps run as one fused launch each on double-buffered
+ * state (every batch without Hz sources), 0 for the split passes. */
 int pfb_info(const pf_batch *b, int64_t *out, int n_out);
 /* The batch's cudaStream_t. */
 void *pfb_stream(pf_batch *b);

@@ -190,11 +190,10 @@ class BatchTE:
     whose stored bytes fit ``memory_budget`` (default: half of the device
     memory free at construction): on a B200 a config-4 batch keeps its whole
     33.5 GB ring and replays nothing; a batch that does not fit gets the
-    memory-minimising K. ``tile_rows`` is the x height of a work tile (4, 8,
-    16 or 32 rows by 32 cells; the marching segments are twice as high);
-    "auto" (the default) lets the autotuner time a short forward chunk at
-    each height on this batch and keep the fastest (``tile_ms_per_step``
-    records the four timings). Results do not depend
+    memory-minimising K. ``tile_rows`` is the x height of a work tile (8, 16
+    or 32 rows by 32 cells); "auto" (the default) lets the autotuner time a
+    short forward chunk at each height on this batch and keep the fastest
+    (``tile_ms_per_step`` records the three timings). Results do not depend
     on the tile height.
     """
 
@@ -244,11 +243,11 @@ class BatchTE:
             self.tile_ms_per_step = None
             self.tile_rows = 32 if auto else int(tile_rows)
             if auto:
-                ms = (C.c_float * 4)()
+                ms = (C.c_float * 3)()
                 best = C.c_int(0)
                 self._chk(L.pfb_tune_tiles(h, int(tune_steps), ms, C.byref(best)))
                 self.tile_rows = int(best.value)
-                self.tile_ms_per_step = {r: float(m) for r, m in zip((4, 8, 16, 32), ms)}
+                self.tile_ms_per_step = {r: float(m) for r, m in zip((8, 16, 32), ms)}
         except Exception:
             self.close()
             raise
@@ -367,11 +366,10 @@ class BatchTE:
         return out
 
     def info(self) -> dict:
-        v = (C.c_int64 * 11)()
-        self._chk(self._L.pfb_info(self.h, v, 11))
+        v = (C.c_int64 * 9)()
+        self._chk(self._L.pfb_info(self.h, v, 9))
         keys = ("cells", "line_cells", "design_cells", "tiles", "checkpoint_every",
-                "segments", "state_reals", "launches", "fused", "march_segments",
-                "bulk_segments")
+                "segments", "state_reals", "launches", "fused")
         return dict(zip(keys, list(v)))
 
     def stream(self) -> int:

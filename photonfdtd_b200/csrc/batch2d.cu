@@ -37,7 +37,6 @@
 #include <map>
 #include <string>
 #include <utility>
-#include <type_traits>
 #include <vector>
 
 #include "../../include/pfb200.h"
@@ -74,14 +73,13 @@ struct pf_batch {
   std::vector<void*> allocs;
   Inst* d_inst = nullptr;
   TileRec* d_tiles = nullptr;
-  SegRec* d_segs = nullptr;   // marching segments: general ones, then bulk ones
+  SegRec* d_segs = nullptr;   // marching segments (forward step)
   int nsegs = 0;
-  int nsegs_general = 0;      // the first nsegs_general segments are not bulk
   size_t seg_cap = 0;         // SegRec slots of d_segs (the shortest segments)
   bool march = true;          // forward step: marching warps (else kb_step tiles)
   int ntiles = 0;
   int tile_rows = 32;
-  size_t tile_cap = 0;  // TileRec slots of d_tiles (the 4-row list, the longest)
+  size_t tile_cap = 0;  // TileRec slots of d_tiles (the 8-row list, the longest)
   void *Ex = nullptr, *Ey = nullptr, *Hz = nullptr, *ce = nullptr;
   // fused step (no H-family sources): a second level of Ex, Ey, Hz and the
   // H psi; the fields after `field_step` steps are in level_at(field_step)
@@ -93,7 +91,6 @@ struct pf_batch {
   void* coef[8] = {};
   void* psi[4] = {};
   int* maps[4] = {};  // mex mhx mey mhy
-  std::vector<int> h_maps[4];  // host copies (pooled), for classifying segments
   void* aE[3] = {};
   void* apsi[4] = {};
   void* g[4] = {};
@@ -255,20 +252,9 @@ void fwd_kernels(pf_batch* b, long long len, bool dft) {
   int pend = 0;
   for (long long t = 0; t < len; ++t) {
     if (b->fused && b->march) {
-      // general segments, then the bulk ones (a separate kernel, more resident)
-      BArgs<T> am = a;
-      am.nsegs = b->nsegs_general;
-      const int nbulk = b->nsegs - b->nsegs_general;
-      if (am.nsegs > 0) {
-        kb_march<T><<<(unsigned)((am.nsegs + kMarchWarps - 1) / kMarchWarps),
-                      dim3(32, kMarchWarps), 0, b->stream>>>(am, (int)t);
-        b->capture_launches += 1;
-      }
-      if (nbulk > 0) {
-        kb_march_bulk<T><<<(unsigned)((nbulk + kMarchWarps - 1) / kMarchWarps),
-                           dim3(32, kMarchWarps), 0, b->stream>>>(am, nbulk, (int)t);
-        b->capture_launches += 1;
-      }
+      kb_march<T><<<(unsigned)((b->nsegs + kMarchWarps - 1) / kMarchWarps), dim3(32, kMarchWarps),
+                    0, b->stream>>>(a, (int)t);
+      b->capture_launches += 1;
     } else if (b->fused) {
       kb_step<T, R><<<G, blk, 0, b->stream>>>(a, (int)t);
       b->capture_launches += 1;
@@ -328,30 +314,15 @@ void adj_kernels(pf_batch* b, long long len) {
   const dim3 blk(32, kWarps);
   const int G = grid_blocks(b);
   if (b->fused && b->march) {
-    // general segments, then the bulk ones (a separate kernel)
-    BArgs<T> am = a;
-    am.nsegs = b->nsegs_general;
-    const int nbulk = b->nsegs - b->nsegs_general;
-    const dim3 mg((unsigned)((am.nsegs + kMarchWarps - 1) / kMarchWarps)), mb(32, kMarchWarps);
-    const dim3 bg((unsigned)((nbulk + kMarchWarps - 1) / kMarchWarps));
-    auto step = [&](auto ht, auto et, int t) {
-      constexpr bool HT = decltype(ht)::value, ET = decltype(et)::value;
-      if (am.nsegs > 0) {
-        kb_adj_march<T, HT, ET><<<mg, mb, 0, b->stream>>>(am, d, t);
-        ++b->capture_launches;
-      }
-      if (nbulk > 0) {
-        kb_adj_march_bulk<T, HT, ET><<<bg, mb, 0, b->stream>>>(am, d, nbulk, t);
-        ++b->capture_launches;
-      }
-    };
-    step(std::false_type{}, std::true_type{}, (int)(len - 1));
+    const dim3 mg((unsigned)((b->nsegs + kMarchWarps - 1) / kMarchWarps)), mb(32, kMarchWarps);
+    kb_adj_march<T, false, true><<<mg, mb, 0, b->stream>>>(a, d, (int)(len - 1));
     for (long long t = len - 1; t >= 0; --t) {
       if (t > 0)
-        step(std::true_type{}, std::true_type{}, (int)t);
+        kb_adj_march<T, true, true><<<mg, mb, 0, b->stream>>>(a, d, (int)t);
       else
-        step(std::true_type{}, std::false_type{}, 0);
+        kb_adj_march<T, true, false><<<mg, mb, 0, b->stream>>>(a, d, 0);
     }
+    b->capture_launches += 1 + len;
     return;
   }
   if (b->fused) {
@@ -672,29 +643,8 @@ std::vector<TileRec> make_tiles(const pf_batch* b, int tile_rows) {
 
 // The marching segments at a height of seg_rows rows: every instance's
 // strips of 31 owned columns, each cut into row ranges.
-// A bulk segment (kSegBulk) needs none of the marching step's edge logic:
-// its rows i0 - 1 .. i1 - 1 and columns j0 - 1 .. j0 + 31 lie inside the
-// instance away from its faces (every neighbour exists), carry no CPML psi
-// (the four compact maps are -1 there), and it does not meet the design
-// window (no curl samples).
-bool bulk_segment(const pf_batch* b, const Inst& I, int i0, int i1, int j0) {
-  if (i0 < 1 || i1 > I.nx - 1 || j0 < 1 || j0 + kMarchCols >= I.ny) return false;
-  if (b->h_maps[0].empty()) return false;
-  for (int i = i0 - 1; i < i1; ++i)
-    if (b->h_maps[0][I.ox + i] >= 0 || b->h_maps[1][I.ox + i] >= 0) return false;
-  for (int j = j0 - 1; j < j0 + kMarchCols; ++j)
-    if (b->h_maps[2][I.oy + j] >= 0 || b->h_maps[3][I.oy + j] >= 0) return false;
-  const bool rows_apart = i1 <= I.di0 || i0 - 1 >= I.di0 + I.dn;
-  const bool cols_apart = j0 + kMarchCols - 1 <= I.dj0 || j0 - 1 >= I.dj0 + I.dn;
-  return rows_apart || cols_apart;
-}
-
-// Segments with the general ones first and the bulk ones (kSegBulk) after
-// them; *n_general receives the count of the first group. Env
-// PFB200_MARCH_NOBULK=1 classifies none as bulk.
-std::vector<SegRec> make_segs(const pf_batch* b, int seg_rows, int* n_general = nullptr) {
-  std::vector<SegRec> gen, bulk;
-  const bool use_bulk = !getenv("PFB200_MARCH_NOBULK");
+std::vector<SegRec> make_segs(const pf_batch* b, int seg_rows) {
+  std::vector<SegRec> segs;
   for (int k = 0; k < b->n_inst; ++k) {
     const Inst& I = b->inst[k];
     for (int j0 = 0; j0 < I.ny; j0 += kMarchCols)
@@ -704,13 +654,10 @@ std::vector<SegRec> make_segs(const pf_batch* b, int seg_rows, int* n_general = 
         sg.i0 = i0;
         sg.i1 = std::min(I.nx, i0 + seg_rows);
         sg.j0 = j0;
-        sg.flags = use_bulk && bulk_segment(b, I, sg.i0, sg.i1, j0) ? kSegBulk : 0;
-        (sg.flags & kSegBulk ? bulk : gen).push_back(sg);
+        segs.push_back(sg);
       }
   }
-  if (n_general) *n_general = (int)gen.size();
-  gen.insert(gen.end(), bulk.begin(), bulk.end());
-  return gen;
+  return segs;
 }
 
 int set_tile_rows(pf_batch* b, int tile_rows) {
@@ -719,13 +666,11 @@ int set_tile_rows(pf_batch* b, int tile_rows) {
   B_CUDA(b, cudaMemcpyAsync(b->d_tiles, tiles.data(), tiles.size() * sizeof(TileRec),
                             cudaMemcpyHostToDevice, b->stream));
   // the marching steps' segments are 2 x tile_rows rows high
-  int n_general = 0;
-  const std::vector<SegRec> segs = make_segs(b, 2 * tile_rows, &n_general);
+  const std::vector<SegRec> segs = make_segs(b, 2 * tile_rows);
   if (segs.size() > b->seg_cap) return bfail(b, PF_ERR_INVALID, "segment list exceeds its buffer");
   B_CUDA(b, cudaMemcpyAsync(b->d_segs, segs.data(), segs.size() * sizeof(SegRec),
                             cudaMemcpyHostToDevice, b->stream));
   b->nsegs = (int)segs.size();
-  b->nsegs_general = n_general;
   B_CUDA(b, cudaStreamSynchronize(b->stream));  // before `tiles` and `segs` go
   destroy_graphs(b);  // captured with the old grid and row count
   b->ntiles = (int)tiles.size();
@@ -736,13 +681,13 @@ int set_tile_rows(pf_batch* b, int tile_rows) {
 
 template <typename T>
 int tune_tiles_t(pf_batch* b, int trial, float* ms3, int* best) {
-  static const int cand[4] = {4, 8, 16, 32};
+  static const int cand[3] = {8, 16, 32};
   cudaEvent_t ev[2] = {nullptr, nullptr};
   int rc = PF_OK;
   if (cudaEventCreate(&ev[0]) != cudaSuccess || cudaEventCreate(&ev[1]) != cudaSuccess)
     rc = bfail(b, PF_ERR_CUDA, "cudaEventCreate failed");
-  int bi = 3;
-  for (int c = 0; c < 4 && !rc; ++c) {
+  int bi = 2;
+  for (int c = 0; c < 3 && !rc; ++c) {
     if ((rc = set_tile_rows(b, cand[c]))) break;
     for (int rep = 0; rep < 2 && !rc; ++rep) {  // rep 0 captures the chunk's graph
       if ((rc = zero_state(b)) || (rc = set_base(b, 0))) break;
@@ -787,8 +732,8 @@ extern "C" {
 int pfb_set_tile_rows(pf_batch* b, int tile_rows) {
   if (!b) return PF_ERR_INVALID;
   if (!b->finalized) return bfail(b, PF_ERR_STATE, "pfb_set_tile_rows before pfb_finalize");
-  if (tile_rows != 4 && tile_rows != 8 && tile_rows != 16 && tile_rows != 32)
-    return bfail(b, PF_ERR_INVALID, "tile_rows must be 4, 8, 16 or 32");
+  if (tile_rows != 8 && tile_rows != 16 && tile_rows != 32)
+    return bfail(b, PF_ERR_INVALID, "tile_rows must be 8, 16 or 32");
   return set_tile_rows(b, tile_rows);
 }
 
@@ -806,8 +751,8 @@ int pfb_finalize(pf_batch* b, int checkpoint_every, int tile_rows) {
   if (!b) return PF_ERR_INVALID;
   if (b->finalized) return bfail(b, PF_ERR_STATE, "pfb_finalize called twice");
   if (checkpoint_every < 0) return bfail(b, PF_ERR_INVALID, "checkpoint_every must be >= 0");
-  if (tile_rows != 4 && tile_rows != 8 && tile_rows != 16 && tile_rows != 32)
-    return bfail(b, PF_ERR_INVALID, "tile_rows must be 4, 8, 16 or 32");
+  if (tile_rows != 8 && tile_rows != 16 && tile_rows != 32)
+    return bfail(b, PF_ERR_INVALID, "tile_rows must be 8, 16 or 32");
   if (b->n_freq < 1) return bfail(b, PF_ERR_STATE, "pfb_set_dft must come before pfb_finalize");
   for (int k = 0; k < b->n_inst; ++k)
     if (b->inst[k].nx == 0) return bfail(b, PF_ERR_STATE, "instance %d not set", k);
@@ -866,9 +811,8 @@ int pfb_finalize(pf_batch* b, int checkpoint_every, int tile_rows) {
     b->nline += I.ny;
     std::vector<char>().swap(b->h_ce[k]);
   }
-  for (int q = 0; q < 4; ++q) b->h_maps[q] = mp[q];
   tiles = make_tiles(b, tile_rows);
-  b->tile_cap = make_tiles(b, 4).size();
+  b->tile_cap = make_tiles(b, 8).size();
   if ((long long)b->tile_cap >= (1LL << 31)) return bfail(b, PF_ERR_INVALID, "too many tiles");
   b->ntiles = (int)tiles.size();
   b->tile_rows = tile_rows;
@@ -878,12 +822,10 @@ int pfb_finalize(pf_batch* b, int checkpoint_every, int tile_rows) {
   B_CUDA(b, cudaMemcpyAsync(b->d_tiles, tiles.data(), tiles.size() * sizeof(TileRec),
                             cudaMemcpyHostToDevice, b->stream));
   {
-    int n_general = 0;
-    const std::vector<SegRec> segs = make_segs(b, 2 * tile_rows, &n_general);
-    b->seg_cap = make_segs(b, 8).size();
+    const std::vector<SegRec> segs = make_segs(b, 2 * tile_rows);
+    b->seg_cap = make_segs(b, 16).size();
     if ((long long)b->seg_cap >= (1LL << 31)) return bfail(b, PF_ERR_INVALID, "too many segments");
     b->nsegs = (int)segs.size();
-    b->nsegs_general = n_general;
     if ((rc = balloc(b, (void**)&b->d_segs, b->seg_cap * sizeof(SegRec)))) return rc;
     B_CUDA(b, cudaMemcpyAsync(b->d_segs, segs.data(), segs.size() * sizeof(SegRec),
                               cudaMemcpyHostToDevice, b->stream));
@@ -1054,18 +996,16 @@ int pfb_read_field(pf_batch* b, int k, int comp, void* dst) {
 
 int pfb_info(const pf_batch* b, int64_t* out, int n_out) {
   if (!b || !out) return PF_ERR_INVALID;
-  const int64_t v[11] = {b->ncell_real,
-                         b->nline,
-                         b->n_design,
-                         b->ntiles,
-                         (int64_t)b->ckpt,
-                         (int64_t)((b->n_steps + b->ckpt - 1) / b->ckpt),
-                         b->state_elems,
-                         b->launches,
-                         b->fused ? 1 : 0,
-                         b->nsegs,
-                         b->nsegs - b->nsegs_general};
-  for (int q = 0; q < n_out && q < 11; ++q) out[q] = v[q];
+  const int64_t v[9] = {b->ncell_real,
+                        b->nline,
+                        b->n_design,
+                        b->ntiles,
+                        (int64_t)b->ckpt,
+                        (int64_t)((b->n_steps + b->ckpt - 1) / b->ckpt),
+                        b->state_elems,
+                        b->launches,
+                        b->fused ? 1 : 0};
+  for (int q = 0; q < n_out && q < 9; ++q) out[q] = v[q];
   return PF_OK;
 }
 

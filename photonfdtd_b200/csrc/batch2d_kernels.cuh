@@ -35,12 +35,6 @@ constexpr int kWarps = 8;     // warps per block
 #ifndef PFB_MINB_MARCH
 #define PFB_MINB_MARCH 12
 #endif
-#ifndef PFB_MINB_MBULK
-#define PFB_MINB_MBULK 16
-#endif
-#ifndef PFB_MINB_ABULK
-#define PFB_MINB_ABULK 10
-#endif
 #ifndef PFB_MINB_AMARCH
 #define PFB_MINB_AMARCH 10
 #endif
@@ -73,9 +67,7 @@ struct __align__(16) TileRec {
 // Its warp's lane l holds column j0 - 1 + l: lane 0 is the halo column.
 struct SegRec {
   int k, i0, i1, j0;
-  int flags;  // kSegBulk: no faces, CPML or design window within reach
 };
-constexpr int kSegBulk = 1;
 constexpr int kMarchCols = 31;  // owned columns per warp
 constexpr int kMarchWarps = 4;  // warps (segments) per block
 
@@ -432,71 +424,6 @@ __global__ void __launch_bounds__(32 * kWarps, PFB_MINB_STEP) kb_step(
 // written, so segments never race, and every cell's arithmetic is kb_h's and
 // kb_e's (hz_value and the E update below), bit for bit. No shared memory,
 // no barriers, about four cell loads and three stores per cell and step.
-// kb_march's row loop for a bulk segment (kSegBulk): every lane's column and
-// both neighbours exist, no psi, no design-window samples, so the loop keeps
-// only the loads, the two curl updates and the stores. Same operations as
-// the general loop on those cells, bit for bit.
-template <typename T>
-__device__ __forceinline__ void march_bulk(const BArgs<T>& a, const SegRec& sg, const Inst& I,
-                                           const T* Ex, const T* Ey, const T* Hz, T* Exo,
-                                           T* Eyo, T* Hzo) {
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x;
-  const long long pitch = I.pitch;
-  const bool own = lane >= 1;
-  const T mch = -a.ch;
-  long long id = I.off + (sg.j0 - 1 + lane) + (long long)(sg.i0 - 1) * pitch;  // row i0 - 1
-  T ex = Ex[id], hz = Hz[id], ey = Ey[id], eyn = Ey[id + pitch];
-  T ex31 = lane == 31 ? Ex[id + 1] : T(0);
-  T K = T(0);
-  T hz_prev = T(0);
-  for (int r = sg.i0 - 1; r < sg.i1; ++r, id += pitch) {
-    T ex_n = T(0), hz_n = T(0), eyn_n = T(0), K_n = T(0), ex31_n = T(0);
-    if (r + 1 < sg.i1) {
-      const long long idn = id + pitch;
-      ex_n = Ex[idn];
-      hz_n = Hz[idn];
-      eyn_n = Ey[idn + pitch];
-      K_n = a.ce[idn];
-      if (lane == 31) ex31_n = Ex[idn + 1];
-    }
-    T exr = __shfl_down_sync(full, ex, 1);
-    if (lane == 31) exr = ex31;
-    T dA, dB;
-    qdiv2(sub_rn(eyn, ey), a.dx, a.rdx, a.fdx, sub_rn(exr, ex), a.dy, a.rdy, a.fdy, dA, dB);
-    const T h = add_rn(hz, mul_rn(sub_rn(dA, dB), mch));
-    const T hl = __shfl_up_sync(full, h, 1);
-    if (r >= sg.i0 && own) {
-      Hzo[id] = h;
-      T qa, qb;
-      qdiv2(sub_rn(h, hl), a.dy, a.rdy, a.fdy, sub_rn(h, hz_prev), a.dx, a.rdx, a.fdx, qa, qb);
-      Exo[id] = add_rn(ex, mul_rn(qa, K));
-      Eyo[id] = add_rn(ey, mul_rn(-qb, K));
-    }
-    hz_prev = h;
-    ex = ex_n;
-    hz = hz_n;
-    ey = eyn;
-    eyn = eyn_n;
-    K = K_n;
-    ex31 = ex31_n;
-  }
-}
-
-// The marching forward step over the bulk segments (the list's tail from
-// a.nsegs on, nbulk of them), compiled for more resident blocks than kb_march.
-template <typename T>
-__global__ void __launch_bounds__(32 * kMarchWarps, PFB_MINB_MBULK) kb_march_bulk(
-    const __grid_constant__ BArgs<T> a, int nbulk, int step_t) {
-  const int w = blockIdx.x * kMarchWarps + threadIdx.y;
-  if (w >= nbulk) return;  // uniform over the warp
-  const SegRec sg = a.segs[a.nsegs + w];
-  const Inst& I = a.inst[sg.k];
-  const long long n = *a.base + step_t;
-  const int L = (int)(n & 1);
-  march_bulk<T>(a, sg, I, a.Ex2[L], a.Ey2[L], a.Hz2[L], a.Ex2[L ^ 1], a.Ey2[L ^ 1], a.Hz2[L ^ 1]);
-}
-
 template <typename T>
 __global__ void __launch_bounds__(32 * kMarchWarps, PFB_MINB_MARCH) kb_march(
     const __grid_constant__ BArgs<T> a, int step_t) {
@@ -1106,111 +1033,6 @@ __global__ void __launch_bounds__(32 * kWarps, PFB_MINB_ASTEP) kb_adj_step(
 // (lane 0 recomputes the halo column's H transpose without storing it). A
 // segment that starts below row 0 first recomputes hA of row i0 - 1. Same
 // levels and arithmetic as kb_adj_step, so the same bits.
-// kb_adj_march's row loop for a bulk segment (kSegBulk): every neighbour
-// exists, no psi adjoints, no design cells; the output line's adjoint source
-// stays. Same operations as the general loop on those cells, bit for bit.
-template <typename T, bool HT, bool ET>
-__device__ __forceinline__ void adj_march_bulk(const BArgs<T>& a, const AArgs<T>& d,
-                                               const SegRec& sg, const Inst& I, long long n) {
-  const long long m = HT ? n - 1 : n;
-  const int lg = (int)(n & 1);
-  const int lh = (int)((n + 1) & 1);
-  const T* gA = d.gA2[lg];
-  const T* gB = d.gB2[lg];
-  T* gAo = d.gA2[(int)(m & 1)];
-  T* gBo = d.gB2[(int)(m & 1)];
-  const T* aHz = d.aHz2[lh];
-  T* aHzo = d.aHz2[lh ^ 1];
-  const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x;
-  const long long pitch = I.pitch;
-  const bool own = lane >= 1;
-  const int j = sg.j0 - 1 + lane;
-  const int r_first = HT ? sg.i0 - 1 : sg.i0;
-  long long id = I.off + j + (long long)r_first * pitch;
-  T ah = T(0), ga = T(0), ga31 = T(0), gb = T(0), gbn = T(0), lx, ly, K = T(0);
-  if (HT) {
-    ah = aHz[id];
-    ga = gA[id];
-    gb = gB[id];
-    gbn = gB[id + pitch];
-    if (lane == 31) ga31 = gA[id + 1];
-  }
-  lx = d.aEx[id];
-  ly = d.aEy[id];
-  if (ET) K = a.ce[id];
-  T ha_prev = T(0);
-  for (int r = r_first; r < sg.i1; ++r, id += pitch) {
-    T ah_n = T(0), ga_n = T(0), ga31_n = T(0), gbn_n = T(0), lx_n = T(0), ly_n = T(0), K_n = T(0);
-    if (r + 1 < sg.i1) {
-      const long long idn = id + pitch;
-      if (HT) {
-        ah_n = aHz[idn];
-        ga_n = gA[idn];
-        gbn_n = gB[idn + pitch];
-        if (lane == 31) ga31_n = gA[idn + 1];
-      }
-      lx_n = d.aEx[idn];
-      ly_n = d.aEy[idn];
-      if (ET) K_n = a.ce[idn];
-    }
-    const bool body = r >= sg.i0;  // uniform
-    T ha = T(0), hb = T(0);
-    if (HT) {
-      T ga1 = __shfl_down_sync(full, ga, 1);
-      if (lane == 31) ga1 = ga31;
-      const T h = fma_rn(sub_rn(gb, gbn), a.idx, fma_rn(sub_rn(ga, ga1), a.idy, ah));
-      ha = mul_rn(-a.ch, h);
-      hb = mul_rn(a.ch, h);
-      if (own && body) aHzo[id] = h;
-    }
-    const T hbl = HT ? __shfl_up_sync(full, hb, 1) : T(0);  // hB of column j - 1
-    if (body && own) {
-      T x = lx, y = ly;
-      if (HT) {
-        y = fma_rn(sub_rn(ha_prev, ha), a.idx, y);
-        x = fma_rn(sub_rn(hbl, hb), a.idy, x);
-      }
-      if (ET) {
-        if (r == I.line_i) {
-          const double* ph = d.phase + m * d.n_freq * 2;
-          const double* g = d.cot + (I.loff + j) * d.n_freq * 2;
-          double sum = 0.0;
-          for (int f = 0; f < d.n_freq; ++f)
-            sum = __dadd_rn(sum, __dadd_rn(__dmul_rn(g[2 * f], ph[2 * f]),
-                                           __dmul_rn(g[2 * f + 1], ph[2 * f + 1])));
-          y = (T)__dadd_rn((double)y, __dmul_rn(d.dt, sum));
-        }
-        gAo[id] = mul_rn(K, x);
-        gBo[id] = mul_rn(-K, y);
-      }
-      d.aEx[id] = x;
-      d.aEy[id] = y;
-    }
-    ha_prev = ha;
-    ah = ah_n;
-    ga = ga_n;
-    ga31 = ga31_n;
-    gb = gbn;
-    gbn = gbn_n;
-    lx = lx_n;
-    ly = ly_n;
-    K = K_n;
-  }
-}
-
-// The marching reverse step over the bulk segments (the list's tail from
-// a.nsegs on, nbulk of them).
-template <typename T, bool HT, bool ET>
-__global__ void __launch_bounds__(32 * kMarchWarps, PFB_MINB_ABULK) kb_adj_march_bulk(
-    const __grid_constant__ BArgs<T> a, const __grid_constant__ AArgs<T> d, int nbulk,
-    int step_t) {
-  const int w = blockIdx.x * kMarchWarps + threadIdx.y;
-  if (w >= nbulk) return;  // uniform over the warp
-  const SegRec sg = a.segs[a.nsegs + w];
-  adj_march_bulk<T, HT, ET>(a, d, sg, a.inst[sg.k], *a.base + step_t);
-}
-
 template <typename T, bool HT, bool ET>
 __global__ void __launch_bounds__(32 * kMarchWarps, PFB_MINB_AMARCH) kb_adj_march(
     const __grid_constant__ BArgs<T> a, const __grid_constant__ AArgs<T> d, int step_t) {
