@@ -590,9 +590,10 @@ def adjoint3d_bench(n: int = 192, n_steps: int = 2000) -> dict:
     """value_and_grad_eps of one 3D scene (photonfdtd_b200.adjoint): n^3
     cells at 20 nm with a 12-cell CPML, float32, four dielectric boxes, an Ex
     dipole, an Ex / Ey DFT on the z = 0 plane at 4 wavelengths, J = sum |DFT|^2.
-    Times the forward run alone and the full gradient (forward with
-    checkpoints, then per segment a replay and the reverse steps), wall
-    clock around synchronised calls."""
+    Times the forward run alone (the faster of two runs) and the full
+    gradient (forward with checkpoints, then per segment a replay and the
+    reverse steps), wall clock around synchronised calls, both from the
+    host scene (tables and engine creation included)."""
     import time
     import torch
     import photonfdtd_b200 as pf
@@ -620,11 +621,13 @@ def adjoint3d_bench(n: int = 192, n_steps: int = 2000) -> dict:
         return sum((v.abs() ** 2).sum() for v in out["dft"]["d"].values())
 
     run_b200(sim)  # warm-up (tables, module load)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    run_b200(sim)
-    torch.cuda.synchronize()
-    t_fwd = time.perf_counter() - t0
+    t_fwd = float("inf")
+    for _ in range(2):  # the faster of two forward runs
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        run_b200(sim)
+        torch.cuda.synchronize()
+        t_fwd = min(t_fwd, time.perf_counter() - t0)
     t0 = time.perf_counter()
     val, g = value_and_grad_eps(sim, loss)
     torch.cuda.synchronize()

@@ -502,6 +502,29 @@ int pfs_mse(int64_t rows, int used, int ld, const float *y, const float *t, floa
 int pfs_adam(int64_t n, float *w, const float *g, float *m, float *v, float lr, float b1,
              float b2, float eps, int step, float wd, void *w16, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Waveguide mode operator (pfm_*), for the GPU mode solver
+ * (photonfdtd_b200/mode.py), replacing the reference's scipy assembly of the
+ * full-vectorial transverse-E operator (src/photonfdtd/mode.py:256-286) and
+ * the operator products of its ARPACK eigensolve (:294-297). All pointers
+ * are device pointers, doubles; calls are asynchronous on `stream` and
+ * allocate nothing. Cross-section ny x nz, flat index iy * nz + iz; a block
+ * holds nvec vectors of 2 * ny * nz values each, [E_z; E_y] as the
+ * reference orders its unknowns; eps: ny * nz relative permittivities;
+ * k2 = (2 pi / wavelength)^2. Error text: pfm_last_error().
+ * ---------------------------------------------------------------------- */
+const char *pfm_last_error(void);
+/* y = P x for the block (x != y). work: 6 * ny * nz * nvec doubles. */
+int pfm_apply(int ny, int nz, double dy, double dz, double k2, const double *eps,
+              const double *x, double *y, int nvec, double *work, void *stream);
+/* x <- T_degree((P - c) / e) x in place, the Chebyshev polynomial of the
+ * first kind mapped so that [lo, hi] goes to [-1, 1] (c, e its centre and
+ * half width): it damps the part of the spectrum in [lo, hi] and amplifies
+ * what lies above hi. work: 10 * ny * nz * nvec doubles. */
+int pfm_chebyshev(int ny, int nz, double dy, double dz, double k2, const double *eps,
+                  double *x, int nvec, int degree, double lo, double hi, double *work,
+                  void *stream);
+
 #ifdef __cplusplus
 }
 #endif

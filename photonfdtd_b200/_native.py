@@ -119,6 +119,11 @@ SIGNATURES = {
     "pfd_density_forward": (C.c_int, [C.c_int, C.c_int, _vp, _dbl, _dbl, _dbl, _vp, _vp]),
     "pfd_density_backward": (C.c_int, [C.c_int, C.c_int, _vp, _dbl, _dbl, _dbl, _vp, _vp,
                                        _vp]),
+    "pfm_last_error": (C.c_char_p, []),
+    "pfm_apply": (C.c_int, [C.c_int, C.c_int, _dbl, _dbl, _dbl, _vp, _vp, _vp, C.c_int, _vp,
+                            _vp]),
+    "pfm_chebyshev": (C.c_int, [C.c_int, C.c_int, _dbl, _dbl, _dbl, _vp, _vp, C.c_int, C.c_int,
+                                _dbl, _dbl, _vp, _vp]),
     "pfs_im2col": (C.c_int, [C.c_int] * 9 + [_vp, _vp, C.c_int, _vp]),
     "pfs_col2im": (C.c_int, [C.c_int] * 9 + [_vp, C.c_int, _vp, _vp]),
     "pfs_bias_act": (C.c_int, [_i64, C.c_int, _vp, _vp, C.c_int, _vp, _vp, _vp]),

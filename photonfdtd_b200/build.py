@@ -25,7 +25,8 @@ def nvcc() -> str:
 def build(debug: bool = False, verbose: bool = False) -> str:
     out = os.path.join(HERE, "libpfb200.so")
     src = [os.path.join(CSRC, f) for f in ("engine.cu", "flux_noalloc.cu", "batch2d.cu",
-                                           "surrogate.cu", "smoothing.cu", "design.cu")]
+                                           "surrogate.cu", "smoothing.cu", "design.cu",
+                                           "modesolver.cu")]
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + \
         [os.path.join(os.path.dirname(HERE), "include", "pfb200.h")]
     if os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(d) for d in deps):
