@@ -77,6 +77,8 @@ def parse():
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-adjoint3d", action="store_true",
                    help="skip the single-scene 3D gradient leg")
+    p.add_argument("--no-mode", action="store_true", help="skip the mode-solver leg")
+    p.add_argument("--only-mode", action="store_true", help="print only the mode-solver leg")
     p.add_argument("--only-adjoint3d", action="store_true",
                    help="print only the single-scene 3D gradient leg")
     p.add_argument("--adjoint-iters", type=int, default=2)
@@ -645,6 +647,45 @@ def adjoint3d_bench(n: int = 192, n_steps: int = 2000) -> dict:
             "finite": bool(np.isfinite(g).all()), "value": float(val)}
 
 
+def mode_bench() -> dict:
+    """The GPU mode solver (photonfdtd_b200.mode) against the reference's
+    scipy ARPACK solver (baseline/_ref) on the reference's high-contrast
+    acceptance case: a 0.3 um n = 3 slab in air, 8 um x 2 um cross-section at
+    0.1 x 0.01 um (80 x 200 cells, 32,000 unknowns), 26 modes at 1.55 um."""
+    import time
+    import torch
+    import photonfdtd_b200 as pf
+    from photonfdtd_b200.mode import ModeSolver
+
+    def build(mod):
+        m = mod or pf
+        core = m.Box(center=(0.0, 0.0), size=(24e-6, 0.3e-6), medium=m.Medium.from_index(3.0))
+        kw = dict(size=(8e-6, 2e-6), cell_size=(0.1e-6, 0.01e-6), structures=[core],
+                  wavelength=1.55e-6, background_eps=1.0, num_modes=26)
+        return mod.ModeSolver(**kw) if mod is not None else ModeSolver(**kw)
+
+    build(None).solve()  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = build(None).solve()
+    torch.cuda.synchronize()
+    t_gpu = time.perf_counter() - t0
+    out = {"workload": "26 modes of a 0.3 um n=3 slab, 80 x 200 cells (32,000 unknowns)",
+           "gpu_s": round(t_gpu, 3), "iterations": int(res.iterations),
+           "max_residual": float(res.max_residual)}
+    try:
+        from baseline.locate import import_reference
+        ref = import_reference()
+    except Exception:  # noqa: BLE001
+        ref = None
+    if ref is not None:
+        t0 = time.perf_counter()
+        rres = build(ref).solve()
+        out["reference_cpu_s"] = round(time.perf_counter() - t0, 3)
+        out["n_eff_max_rel_diff"] = float(np.max(np.abs(res.n_eff - rres.n_eff) / rres.n_eff))
+    return out
+
+
 def adjoint_cpu_baseline(sim, win, cells_total, steps=60):
     """The NumPy forward + adjoint restatement (oracle/adjoint2d.py) on the
     first instance for `steps` steps, scaled by cell-steps to the batch."""
@@ -664,6 +705,9 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.only_mode:
+        print(json.dumps(mode_bench()), flush=True)
+        return
     if args.only_adjoint3d:
         print(json.dumps(adjoint3d_bench()), flush=True)
         return
@@ -772,6 +816,8 @@ def main():
         line["adjoint"] = adj
     if rank == 0 and world == 1 and not args.no_adjoint3d:
         line["adjoint3d"] = adjoint3d_bench()
+    if rank == 0 and world == 1 and not args.no_mode:
+        line["mode_solver"] = mode_bench()
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         line["reference_gpu"] = reference_gpu_bench(args.size)
     if rank == 0 and world == 1 and not args.no_surrogate:
