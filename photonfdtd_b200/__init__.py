@@ -16,7 +16,9 @@ arguments), and ``photonfdtd_b200.plugin.install()`` registers
 """
 from .scene import (C_0, EPS_0, ETA_0, MU_0, Q_E, VACUUM, Box, CPMLParams, DFTMonitor,
                     DispersiveMedium, FieldMonitor, FluxMonitor, GaussianPulse, Grid, Medium,
-                    ModeSource, PointDipole, Pole, cpml_coeffs_1axis)
+                    ModeSource, PointDipole, Pole, UniModeSource, cpml_coeffs_1axis)
+from .mode import ModeResult, ModeSolver
+from .smatrix import mode_amplitudes, s_parameters
 from .simulation import Result, Simulation
 from .smoothing import smooth_permittivity
 
@@ -25,6 +27,7 @@ __version__ = "0.1.0"
 __all__ = [
     "C_0", "EPS_0", "ETA_0", "MU_0", "Q_E", "VACUUM", "Box", "CPMLParams", "DFTMonitor",
     "DispersiveMedium", "FieldMonitor", "FluxMonitor", "GaussianPulse", "Grid", "Medium",
-    "ModeSource", "PointDipole", "Pole", "cpml_coeffs_1axis", "Result", "Simulation",
+    "ModeSource", "PointDipole", "Pole", "UniModeSource", "ModeResult", "ModeSolver",
+    "cpml_coeffs_1axis", "Result", "Simulation", "mode_amplitudes", "s_parameters",
     "smooth_permittivity",
 ]

@@ -383,6 +383,57 @@ class ModeSource:
         return out
 
 
+@dataclass(frozen=True)
+class UniModeSource:
+    """One-way launch of a solved waveguide mode along x (sources.py:341-433):
+    an electric and a magnetic current sheet on the same plane (the
+    equivalence principle: J = x x H_m, M = -x x E_m), whose radiation adds
+    in ``direction`` and cancels behind it. ``mode`` is a ModeResult solved
+    on the plane's own (y, z) cells; each cell becomes four soft dipoles,
+        Ey: C Hz / (eps0 eps_r),  Ez: -C Hy / (eps0 eps_r),
+        Hy: -s C Ez / mu0,        Hz:  s C Ey / mu0,
+    with s = +1 for "+x", -1 for "-x", C = ``amplitude``, the mode's fields
+    first rotated so that its largest transverse E entry is real, then taken
+    real. Each mode cell maps to the nearest grid cell of the plane."""
+    center: Tuple[float, float, float]
+    size: Tuple[float, float, float]
+    waveform: GaussianPulse
+    mode: object
+    mode_index: int = 0
+    direction: str = "+x"
+    amplitude: float = 1.0
+
+    def expand(self, grid: Grid) -> List[PointDipole]:
+        if self.direction not in ("+x", "-x"):
+            raise ValueError("UniModeSource supports direction '+x' or '-x'")
+        sgn = 1.0 if self.direction == "+x" else -1.0
+        cen = list(self.center) + [0.0] * (3 - len(self.center))
+        m, q = self.mode, self.mode_index
+        ey, ez = np.asarray(m.Ey[q]), np.asarray(m.Ez[q])
+        hy, hz = np.asarray(m.Hy[q]), np.asarray(m.Hz[q])
+        peak = int(np.argmax(np.abs(ey) + np.abs(ez)))
+        rot = np.exp(-1j * np.angle((ey.ravel() + ez.ravel())[peak]))
+        ey, ez, hy, hz = (np.real(f * rot) for f in (ey, ez, hy, hz))
+        eps = np.asarray(m.eps_r)
+        amp = float(self.amplitude)
+        sheets = (("Ey", amp / (EPS_0 * eps) * hz), ("Ez", -amp / (EPS_0 * eps) * hy),
+                  ("Hy", -sgn * amp / MU_0 * ez), ("Hz", sgn * amp / MU_0 * ey))
+        xc, yc, zc = grid.coords
+        x = float(xc[int(np.argmin(np.abs(xc - cen[0])))] if xc.size > 1 else cen[0])
+        out = []
+        for jy, yv in enumerate(np.asarray(m.y)):
+            y = float(yc[int(np.argmin(np.abs(yc - (cen[1] + yv))))] if yc.size > 1 else cen[1])
+            for jz, zv in enumerate(np.asarray(m.z)):
+                z = float(zc[int(np.argmin(np.abs(zc - (cen[2] + zv))))]
+                          if zc.size > 1 else cen[2])
+                for comp, a in sheets:
+                    v = float(a[jy, jz])
+                    if v != 0.0:
+                        out.append(PointDipole(position=(x, y, z), component=comp,
+                                               waveform=self.waveform, amplitude=v))
+        return out
+
+
 # --------------------------------------------------------------------------- #
 # Monitors
 # --------------------------------------------------------------------------- #

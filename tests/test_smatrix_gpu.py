@@ -7,7 +7,9 @@ functions applied to the same arrays (1e-12), and |alpha+|^2 at the first
 frequency, as a loss of the engine run's DFT outputs, is differentiated with
 respect to eps_r by the engine's adjoint and by the oracle's transposed step
 (oracle/adjoint3d.py): the two gradients agree to 1e-10 relative L2
-(float64)."""
+(float64). Then the reference's own end-to-end checks on the engine: |S21|
+of a ModeSource-launched waveguide mode within 0.05 of 1, and the backward
+amplitude of a UniModeSource below 0.3 of the forward one."""
 import numpy as np
 import pytest
 import torch
@@ -91,3 +93,59 @@ def test_s_parameter_gradient_engine_against_oracle():
     assert v == pytest.approx(vo, rel=1e-12)
     assert np.abs(g).max() > 0
     assert np.linalg.norm(g - go) <= 1e-10 * np.linalg.norm(go)
+
+
+# The reference's end-to-end S-parameter checks (tests/test_smatrix.py:88-152,
+# run there on its JAX backend), here on the engine with the GPU mode solver:
+# a silicon strip waveguide (0.45 x 0.22 um, n = 3.48) in a 2 x 1.4 um
+# cross-section at 40 nm, the mode solved with a 1.44^2 background.
+def _wg_mode():
+    core = pf.Box(center=(0, 0), size=(0.45e-6, 0.22e-6), medium=pf.Medium.from_index(3.48))
+    ms = ModeSolver(size=(2.0e-6, 1.4e-6), cell_size=(40e-9, 40e-9), structures=[core],
+                    wavelength=1.55e-6, background_eps=1.44 ** 2, num_modes=2)
+    return ms, ms.solve()
+
+
+def test_waveguide_s21_energy_conserving():
+    """A mode launched down a straight lossless waveguide keeps |S21| ~= 1
+    between two downstream ports (the reference's bound: within 0.05)."""
+    f0 = C_0 / 1.55e-6
+    ms, mr = _wg_mode()
+    core = pf.Box(center=(0, 0, 0), size=(10e-6, 0.45e-6, 0.22e-6),
+                  medium=pf.Medium.from_index(3.48))
+    grid = pf.Grid(size=(6e-6, 2.0e-6, 1.4e-6), cell_size=40e-9, pml_layers=(10, 10, 10))
+    src = pf.ModeSource(center=(-2e-6, 0, 0), size=(0, 2.0e-6, 1.4e-6), component="Ey",
+                        waveform=pf.GaussianPulse(freq0=f0, fwhm=10e-15),
+                        profile=np.real(mr.Ey[0]), profile_coords=(ms.y, ms.z))
+    ports = [pf.DFTMonitor(name=n, components=("Ey", "Ez", "Hy", "Hz"), freqs=[f0],
+                           plane_axis="x", plane_position=x) for n, x in (("p1", 0.0),
+                                                                          ("p2", 2.0e-6))]
+    res = run_b200(pf.Simulation(grid, structures=[core], sources=[src], monitors=ports,
+                                 run_time=200e-15))
+    dA = 40e-9 * 40e-9
+    a1, _ = pf.s_parameters(res, "p1", mr, 0, dA)
+    a2, _ = pf.s_parameters(res, "p2", mr, 0, dA)
+    assert abs(a2[0] / a1[0]) == pytest.approx(1.0, abs=0.05)
+
+
+def test_unidirectional_source_extinction():
+    """UniModeSource launches one way: the backward amplitude upstream is
+    below 0.3 of the forward one downstream (the reference's bound)."""
+    f0 = C_0 / 1.55e-6
+    _, mr = _wg_mode()
+    core = pf.Box(center=(0, 0, 0), size=(12e-6, 0.45e-6, 0.22e-6),
+                  medium=pf.Medium.from_index(3.48))
+    grid = pf.Grid(size=(8e-6, 2.0e-6, 1.4e-6), cell_size=40e-9, pml_layers=(10, 10, 10))
+    src = pf.UniModeSource(center=(0, 0, 0), size=(0, 2.0e-6, 1.4e-6),
+                           waveform=pf.GaussianPulse(freq0=f0, fwhm=10e-15), mode=mr,
+                           direction="+x")
+    ports = [pf.DFTMonitor(name=n, components=("Ey", "Ez", "Hy", "Hz"), freqs=[f0],
+                           plane_axis="x", plane_position=x) for n, x in (("up", -1.5e-6),
+                                                                          ("dn", 1.5e-6))]
+    res = run_b200(pf.Simulation(grid, structures=[core], sources=[src], monitors=ports,
+                                 run_time=220e-15))
+    dA = 40e-9 * 40e-9
+    fwd, _ = pf.s_parameters(res, "dn", mr, 0, dA)
+    _, back = pf.s_parameters(res, "up", mr, 0, dA)
+    assert abs(fwd[0]) > 0
+    assert abs(back[0]) / abs(fwd[0]) < 0.3
