@@ -78,6 +78,9 @@ def parse():
     p.add_argument("--no-adjoint3d", action="store_true",
                    help="skip the single-scene 3D gradient leg")
     p.add_argument("--no-mode", action="store_true", help="skip the mode-solver leg")
+    p.add_argument("--no-batch3d", action="store_true", help="skip the concurrent-scenes leg")
+    p.add_argument("--only-batch3d", action="store_true",
+                   help="print only the concurrent-scenes leg")
     p.add_argument("--only-mode", action="store_true", help="print only the mode-solver leg")
     p.add_argument("--only-adjoint3d", action="store_true",
                    help="print only the single-scene 3D gradient leg")
@@ -686,6 +689,56 @@ def mode_bench() -> dict:
     return out
 
 
+def batch3d_bench(n_scenes: int = 24, n_steps: int = 600) -> dict:
+    """Many small uneven 3D scenes on one GPU (photonfdtd_b200.batch3d):
+    n_scenes grids of 40^3 to 96^3 cells (seeded sizes, 8-cell CPML, two
+    dielectric boxes, an Ez dipole, an Ez DFT plane at 2 wavelengths),
+    float32, n_steps steps each, from host scenes to Results: one after
+    another (run_b200 each) against all at once (run_many), wall clock."""
+    import time
+    import torch
+    import photonfdtd_b200 as pf
+    from photonfdtd_b200.batch3d import run_many
+    from photonfdtd_b200.engine import run_b200
+    rng = np.random.default_rng(11)
+    d, f0 = 40e-9, 299_792_458.0 / 1.2e-6
+
+    def scene(n):
+        L = n * d
+        grid = pf.Grid(size=(L, L, L), cell_size=d, pml_layers=(8, 8, 8))
+        boxes = [pf.Box(center=(0.1 * L, 0.0, 0.0), size=(0.2 * L, 0.3 * L, 0.3 * L),
+                        medium=pf.Medium(permittivity=4.0)),
+                 pf.Box(center=(-0.1 * L, 0.1 * L, 0.0), size=(0.1 * L, 0.2 * L, 0.4 * L),
+                        medium=pf.Medium(permittivity=2.25))]
+        src = pf.PointDipole(position=(-0.25 * L, 0.0, 0.0), component="Ez",
+                             waveform=pf.GaussianPulse(freq0=f0, fwhm=4e-15))
+        mon = pf.DFTMonitor(name="d", components=("Ez",), freqs=[f0, 1.2 * f0],
+                            plane_axis="z", plane_position=0.0)
+        dt = pf.Simulation(grid, structures=boxes, sources=[src], monitors=[mon],
+                           run_time=1e-15).dt
+        return pf.Simulation(grid, structures=boxes, sources=[src], monitors=[mon],
+                             run_time=(n_steps - 0.5) * dt)
+
+    sizes = [int(v) for v in rng.integers(40, 97, n_scenes)]
+    cells = sum(n ** 3 for n in sizes) * n_steps
+    run_many([scene(n) for n in sizes[:2]])  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for n in sizes:
+        run_b200(scene(n))
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    run_many([scene(n) for n in sizes])
+    torch.cuda.synchronize()
+    t_con = time.perf_counter() - t0
+    return {"workload": f"{n_scenes} 3D scenes of 40^3-96^3 cells (seeded), float32, "
+                        f"{n_steps} steps each, host scene to Result",
+            "cell_steps": cells, "sequential_s": round(t_seq, 3),
+            "concurrent_s": round(t_con, 3), "speedup": round(t_seq / t_con, 2),
+            "concurrent_mcell_updates_per_s": round(cells / t_con / 1e6, 1)}
+
+
 def adjoint_cpu_baseline(sim, win, cells_total, steps=60):
     """The NumPy forward + adjoint restatement (oracle/adjoint2d.py) on the
     first instance for `steps` steps, scaled by cell-steps to the batch."""
@@ -705,6 +758,9 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.only_batch3d:
+        print(json.dumps(batch3d_bench()), flush=True)
+        return
     if args.only_mode:
         print(json.dumps(mode_bench()), flush=True)
         return
@@ -816,6 +872,8 @@ def main():
         line["adjoint"] = adj
     if rank == 0 and world == 1 and not args.no_adjoint3d:
         line["adjoint3d"] = adjoint3d_bench()
+    if rank == 0 and world == 1 and not args.no_batch3d:
+        line["batch3d"] = batch3d_bench()
     if rank == 0 and world == 1 and not args.no_mode:
         line["mode_solver"] = mode_bench()
     if rank == 0 and world == 1 and not args.no_reference_gpu:
