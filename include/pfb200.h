@@ -189,8 +189,9 @@ int pf_set_state(pf_engine *eng, int64_t step, const void *src, int64_t bytes,
  * with respect to the per-cell E coefficient K = dt / (eps0 eps_r), i.e. the
  * time-domain adjoint behind value_and_grad_eps
  * (src/photonfdtd/jaxbackend.py:666-722, which differentiates the same step
- * with jax.grad; like it, no dispersive media and no subpixel tensor:
- * PF_ERR_UNSUPPORTED). Protocol, after a forward run that saved pf_get_state
+ * with jax.grad; like it, no dispersive media: PF_ERR_UNSUPPORTED;
+ * per-component coefficients, PF_CE_CELL3, are differentiated component by
+ * component). Protocol, after a forward run that saved pf_get_state
  * checkpoints at the segment starts:
  *   pf_adj_init(ring_steps)     adjoint state + a replay ring of ring_steps
  *                               steps (the longest segment); zeroes the
@@ -221,6 +222,11 @@ int pf_adj_add_field_source(pf_engine *eng, int64_t step, int comp, const int32_
 int pf_adj_segment(pf_engine *eng, int64_t step0, int64_t n, const void *state,
                    int64_t bytes, int state_on_device);
 int pf_adj_read_grad(pf_engine *eng, double *dst);
+/* dJ/dK_c per component and cell (3 * ncell doubles: Ex cells, then Ey,
+ * then Ez): the gradient for per-component coefficients (PF_CE_CELL3, e.g.
+ * a density mapped to an anisotropic permittivity; jaxbackend.py:725-775
+ * value_and_grad_params differentiates the same quantities). */
+int pf_adj_read_grad_components(pf_engine *eng, double *dst);
 
 /* Steps advanced so far. */
 int pf_step(const pf_engine *eng, int64_t *step);

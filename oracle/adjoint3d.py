@@ -30,8 +30,8 @@ class _RecordingRun(OracleRun):
     coefficient multiplies: g = curl + sum(sign * psi') over the update's
     region (psi' the slab's value after the step)."""
 
-    def __init__(self, sim, n_steps=None):
-        super().__init__(sim, n_steps)
+    def __init__(self, sim, n_steps=None, ce3=None):
+        super().__init__(sim, n_steps, ce3=ce3)
         self.g_hist: List[Dict[str, np.ndarray]] = []
 
     def _apply(self, family):
@@ -82,8 +82,23 @@ def forward_value(sim, loss: Callable) -> float:
 
 def value_and_grad_eps(sim, loss: Callable) -> Tuple[float, np.ndarray]:
     """(J, dJ/deps_r) of a loss of the monitor outputs, in float64 numpy."""
+    run, val, gk = _reverse(sim, loss, None)
+    eps = np.asarray(run.t["eps"], np.float64)
+    g = (gk["Ex"] + gk["Ey"]) + gk["Ez"]
+    return val, g * (-run.dt / (EPS0 * eps * eps))
+
+
+def value_and_grad_ce3(sim, ce3, loss: Callable) -> Tuple[float, np.ndarray]:
+    """(J, dJ/dK_c) with the E coefficients of Ex, Ey, Ez given per cell
+    (``ce3``, three grid-shaped arrays): the gradient value_and_grad_params
+    chains to its parameters (jaxbackend.py:725-775), shaped (3, *grid)."""
+    _, val, gk = _reverse(sim, loss, ce3)
+    return val, np.stack([gk["Ex"], gk["Ey"], gk["Ez"]])
+
+
+def _reverse(sim, loss: Callable, ce3):
     import torch
-    run = _RecordingRun(sim)
+    run = _RecordingRun(sim, ce3=ce3)
     run.advance(run.n_steps)
     res = run.result()
     out = _out_dict(res, torch)
@@ -93,7 +108,7 @@ def value_and_grad_eps(sim, loss: Callable) -> Tuple[float, np.ndarray]:
     lam = {c: np.zeros(shape) for c in run.F}
     lpsi = [[[np.zeros(psi.shape) for (_, _, _, psi) in slabs]
              for (_, _, _, _, slabs) in terms] for (_, _, _, _, _, terms) in run.updates]
-    gk = np.zeros(shape)
+    gk = {c: np.zeros(shape) for c in ("Ex", "Ey", "Ez")}
 
     # the loss's sources per step: DFT samples and FieldMonitor frames
     def sources(n):
@@ -142,7 +157,7 @@ def value_and_grad_eps(sim, loss: Callable) -> Tuple[float, np.ndarray]:
         lf = lam[name][reg]
         k = k_arr if is_e else k_sc
         if is_e:
-            gk[reg] += lf * run.g_hist[n][name]
+            gk[name][reg] += lf * run.g_hist[n][name]
         for t, (ax, src, oax, sign, slabs) in enumerate(terms):
             ld = sign * k * lf
             for q, (sl, bb, cc, psi) in enumerate(slabs):
@@ -175,5 +190,4 @@ def value_and_grad_eps(sim, loss: Callable) -> Tuple[float, np.ndarray]:
             transpose(u, n)
         for u in h_upd:
             transpose(u, n)
-    eps = np.asarray(run.t["eps"], np.float64)
-    return float(val.detach()), gk * (-dt / (EPS0 * eps * eps))
+    return run, float(val.detach()), gk

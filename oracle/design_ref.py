@@ -58,3 +58,30 @@ def backward(rho, grad_phys, radius_cells=0.0, beta=0.0, eta=0.5):
     den = convolve(np.ones_like(rho), k, mode="same", method="direct")
     # y = C rho / d with C a symmetric-kernel same-size convolution: C^T = C
     return convolve(g / den, k, mode="same", method="direct")
+
+
+def etched_core_eps(grid, rho, eps_solid, eps_void, eps_sub, eps_clad, core_z,
+                    filter_radius=0.0, beta=0.0, eta=0.5):
+    """(eps_xx, eps_yy, eps_zz) of the reference's EtchedCore.eps_components
+    (design.py:109-148) in NumPy: the physical density, the arithmetic and
+    harmonic means, the in-plane normal from numpy.gradient, the blend along
+    the normal, and the extrusion through the substrate / core / cladding
+    stack."""
+    nx, ny, nz = grid.shape
+    dx = grid.cell_size[0]
+    dy = grid.cell_size[1] if grid.shape[1] > 1 else dx
+    rp = forward(np.asarray(rho, np.float64), filter_radius / dx, beta, eta)
+    eps_a = eps_void + rp * (eps_solid - eps_void)
+    eps_h = 1.0 / (rp / eps_solid + (1.0 - rp) / eps_void)
+    gx = np.gradient(rp, dx, axis=0)
+    gy = np.gradient(rp, dy, axis=1)
+    gmag = np.sqrt(gx ** 2 + gy ** 2)
+    safe = gmag > (gmag.max() * 1e-9 + 1e-30)
+    inv = np.where(safe, 1.0 / np.where(safe, gmag, 1.0), 0.0)
+    nxc, nyc = gx * inv, gy * inv
+    delta = eps_h - eps_a
+    comps = (eps_a + delta * nxc ** 2, eps_a + delta * nyc ** 2, eps_a)
+    zc = np.asarray(grid.coords[2])
+    core = ((zc >= core_z[0]) & (zc < core_z[1])).astype(float).reshape(1, 1, nz)
+    bg = np.where(zc < core_z[0], eps_sub, eps_clad).reshape(1, 1, nz)
+    return tuple(c[:, :, None] * core + bg * (1.0 - core) for c in comps)

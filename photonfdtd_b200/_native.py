@@ -64,6 +64,7 @@ SIGNATURES = {
     "pf_adj_add_field_source": (C.c_int, [_vp, _i64, C.c_int, _pi32, _pi32, _pi32, _pdbl]),
     "pf_adj_segment": (C.c_int, [_vp, _i64, _i64, _vp, _i64, C.c_int]),
     "pf_adj_read_grad": (C.c_int, [_vp, _pdbl]),
+    "pf_adj_read_grad_components": (C.c_int, [_vp, _pdbl]),
     "pf_write_field": (C.c_int, [_vp, C.c_int, _vp]),
     "pf_set_check_every": (C.c_int, [_vp, _i64]),
     "pf_set_wait_test": (C.c_int, [_vp, C.c_int]),

@@ -77,20 +77,11 @@ def _out_dict(res, torch):
     return leaves
 
 
-def value_and_grad_eps(sim, loss: Callable, checkpoint_every: int = None
-                       ) -> Tuple[float, np.ndarray]:
-    """``(value, d value / d eps_r)`` for a scalar ``loss(out)`` of the
-    simulation's monitor outputs (jaxbackend.py:666-722). ``checkpoint_every``
-    is the segment length of the reverse pass (default ceil(sqrt(n_steps)));
-    device memory holds n_steps / checkpoint_every states plus one segment of
-    per-step records (three H fields and the E-side CPML state per step)."""
+def _adjoint(sim, t: dict, loss: Callable, checkpoint_every) -> Tuple[float, np.ndarray]:
+    """The forward run with checkpoints, the loss and its output
+    sensitivities, and the reverse pass: (J, dJ/dK_c) with the per-component
+    gradient shaped (3, *grid) for the E coefficients K of Ex, Ey, Ez."""
     import torch
-    validate(sim)
-    if sim.subpixel or getattr(sim, "_has_dispersion", False):
-        raise NotImplementedError(
-            "value_and_grad_eps differentiates the scalar per-cell eps_r, which does not "
-            "parameterize a subpixel-smoothed tensor or a dispersive pole model.")
-    t = build_tables(sim)
     n_steps, dt = t["n_steps"], t["dt"]
     if n_steps < 1:
         raise ValueError("nothing to differentiate: the simulation has no steps")
@@ -149,11 +140,63 @@ def value_and_grad_eps(sim, loss: Callable, checkpoint_every: int = None
             buf = proxy.ckpts[s0]
             eng._chk(eng._L.pf_adj_segment(eng.h, int(s0), int(n), N.C.c_void_p(buf.data_ptr()),
                                            int(proxy.nbytes), 1))
-        grad_k = np.empty(int(np.prod(t["shape"])), np.float64)
-        eng._chk(eng._L.pf_adj_read_grad(eng.h, N.ptr(grad_k, N.C.c_double)))
+        grad_k = np.empty(3 * int(np.prod(t["shape"])), np.float64)
+        eng._chk(eng._L.pf_adj_read_grad_components(eng.h, N.ptr(grad_k, N.C.c_double)))
     finally:
         eng.close()
+    return value, grad_k.reshape((3,) + tuple(t["shape"]))
+
+
+def _no_dispersion(sim, what: str) -> None:
+    if getattr(sim, "_has_dispersion", False):
+        raise NotImplementedError(f"{what} does not support dispersive media (the pole state "
+                                  "is not parameterized).")
+
+
+def value_and_grad_eps(sim, loss: Callable, checkpoint_every: int = None
+                       ) -> Tuple[float, np.ndarray]:
+    """``(value, d value / d eps_r)`` for a scalar ``loss(out)`` of the
+    simulation's monitor outputs (jaxbackend.py:666-722). ``checkpoint_every``
+    is the segment length of the reverse pass (default ceil(sqrt(n_steps)));
+    device memory holds n_steps / checkpoint_every states plus one segment of
+    per-step records (three H fields and the E-side CPML state per step)."""
+    validate(sim)
+    _no_dispersion(sim, "value_and_grad_eps")
+    if sim.subpixel:
+        raise NotImplementedError(
+            "value_and_grad_eps differentiates the scalar per-cell eps_r, which does not "
+            "parameterize a subpixel-smoothed tensor; use value_and_grad_params.")
+    t = build_tables(sim)
+    value, g3 = _adjoint(sim, t, loss, checkpoint_every)
+    dt = t["dt"]
     eps = np.asarray(sim.eps_r, dtype=np.float64).reshape(t["shape"])
-    # K = dt / (eps0 eps_r)  =>  dK/deps_r = -dt / (eps0 eps_r^2)
-    grad = grad_k.reshape(t["shape"]) * (-dt / (EPS_0 * eps * eps))
+    # K = dt / (eps0 eps_r) for all three components  =>  dK/deps_r = -dt / (eps0 eps_r^2)
+    grad = ((g3[0] + g3[1]) + g3[2]) * (-dt / (EPS_0 * eps * eps))
     return value, grad.astype(np.dtype(sim.dtypes["eps_r"]))
+
+
+def value_and_grad_params(sim, ce_of_params: Callable, params, loss: Callable,
+                          checkpoint_every: int = None):
+    """``(value, d value / d params)`` for design parameters that set the
+    per-component E coefficients (jaxbackend.py:725-775): ``ce_of_params(p)``
+    returns ``{'Ex', 'Ey', 'Ez'}`` grid-shaped torch tensors built from ``p``
+    with torch operations (e.g. photonfdtd_b200.design.EtchedCore.ce_builder);
+    the engine runs with exactly those coefficients, its adjoint gives dJ/dK
+    per component, and torch carries them back to ``params``. ``params`` is a
+    torch tensor (the gradient is returned as one of its dtype and device) or
+    an array (returned as NumPy)."""
+    import torch
+    validate(sim)
+    _no_dispersion(sim, "value_and_grad_params")
+    as_numpy = not torch.is_tensor(params)
+    p = (torch.as_tensor(np.asarray(params, np.float64)) if as_numpy else params).detach()
+    p = p.clone().requires_grad_(True)
+    with torch.enable_grad():
+        ce = ce_of_params(p)
+        comps = [ce[c] for c in ("Ex", "Ey", "Ez")]
+        t = build_tables(sim, ce3=[c.detach().cpu().numpy() for c in comps])
+        value, g3 = _adjoint(sim, t, loss, checkpoint_every)
+        torch.autograd.backward(comps, [torch.as_tensor(g3[i], dtype=c.dtype, device=c.device)
+                                        for i, c in enumerate(comps)])
+    g = p.grad if p.grad is not None else torch.zeros_like(p)
+    return value, (g.cpu().numpy() if as_numpy else g)

@@ -1393,6 +1393,7 @@ AdjState<T> adj_state(pf_engine* e, long long slot) {
     s.lpH[q] = (T*)e->lpH[q];
   }
   s.grad = e->grad;
+  s.ncell = e->ncell;
   for (int a = 0; a < 3; ++a) s.idl[a] = (T)(1.0 / e->dl[a]);
   return s;
 }
@@ -1438,6 +1439,8 @@ int adj_segment_typed(pf_engine* e, long long step0, long long n) {
     if ((rc = adj_sources<T>(e, m, 0))) return rc;
     if (e->ce_mode == PF_CE_CELL1)
       k_adj_e<T, kCeCell1><<<grd, blk, 0, e->stream>>>(a, s);
+    else if (e->ce_mode == PF_CE_CELL3)
+      k_adj_e<T, kCeCell3><<<grd, blk, 0, e->stream>>>(a, s);
     else
       k_adj_e<T, kCeTable><<<grd, blk, 0, e->stream>>>(a, s);
     if ((rc = adj_sources<T>(e, m, 1))) return rc;
@@ -1461,7 +1464,7 @@ int adj_zero(pf_engine* e) {
     if (e->npsiE[q]) PF_CUDA(e, cudaMemsetAsync(e->lpE[q], 0, e->npsiE[q] * S, e->stream));
     if (e->npsiH[q]) PF_CUDA(e, cudaMemsetAsync(e->lpH[q], 0, e->npsiH[q] * S, e->stream));
   }
-  PF_CUDA(e, cudaMemsetAsync(e->grad, 0, (size_t)e->ncell * 8, e->stream));
+  PF_CUDA(e, cudaMemsetAsync(e->grad, 0, (size_t)e->ncell * 24, e->stream));
   PF_CUDA(e, cudaStreamSynchronize(e->stream));
   e->adj_next = e->n_steps;
   return PF_OK;
@@ -1491,9 +1494,6 @@ int pf_adj_init(pf_engine* e, int64_t ring_steps) {
   if (!e->finalized) return fail(e, PF_ERR_STATE, "pf_adj_init before pf_finalize");
   if (e->n_media > 0)
     return fail(e, PF_ERR_UNSUPPORTED, "the adjoint does not cover dispersive (ADE) media");
-  if (e->ce_mode == PF_CE_CELL3)
-    return fail(e, PF_ERR_UNSUPPORTED,
-                "the adjoint differentiates one coefficient per cell, not a subpixel tensor");
   if (ring_steps < 1 || ring_steps > e->n_steps)
     return fail(e, PF_ERR_INVALID, "ring_steps %lld outside [1, n_steps]", (long long)ring_steps);
   PF_CUDA(e, cudaSetDevice(e->device));
@@ -1510,7 +1510,7 @@ int pf_adj_init(pf_engine* e, int64_t ring_steps) {
       if ((rc = dalloc(e, &e->lpE[q], e->npsiE[q] * S))) return rc;
       if ((rc = dalloc(e, &e->lpH[q], e->npsiH[q] * S))) return rc;
     }
-    if ((rc = dalloc(e, (void**)&e->grad, (size_t)e->ncell * 8))) return rc;
+    if ((rc = dalloc(e, (void**)&e->grad, (size_t)e->ncell * 24))) return rc;
     e->dft_cot.assign(e->dfts.size(), nullptr);
     e->adj = true;
   }
@@ -1574,10 +1574,20 @@ int pf_adj_segment(pf_engine* e, int64_t step0, int64_t n, const void* state, in
   return e->rb == 4 ? adj_segment_typed<float>(e, step0, n) : adj_segment_typed<double>(e, step0, n);
 }
 
+int pf_adj_read_grad_components(pf_engine* e, double* dst) {
+  if (!e || !dst) return PF_ERR_INVALID;
+  if (!e->adj) return fail(e, PF_ERR_STATE, "gradient read before pf_adj_init");
+  PF_CUDA(e, cudaMemcpy(dst, e->grad, (size_t)e->ncell * 24, cudaMemcpyDeviceToHost));
+  return PF_OK;
+}
+
 int pf_adj_read_grad(pf_engine* e, double* dst) {
   if (!e || !dst) return PF_ERR_INVALID;
-  if (!e->adj) return fail(e, PF_ERR_STATE, "pf_adj_read_grad before pf_adj_init");
-  PF_CUDA(e, cudaMemcpy(dst, e->grad, (size_t)e->ncell * 8, cudaMemcpyDeviceToHost));
+  std::vector<double> g((size_t)e->ncell * 3);
+  int rc = pf_adj_read_grad_components(e, g.data());
+  if (rc) return rc;
+  const size_t n = (size_t)e->ncell;
+  for (size_t i = 0; i < n; ++i) dst[i] = (g[i] + g[n + i]) + g[2 * n + i];
   return PF_OK;
 }
 

@@ -38,7 +38,8 @@ struct AdjState {
   T* gH[6];   // of the H update: Hx A, Hx B, Hy A, Hy B, Hz A, Hz B
   T* lpE[6];  // psi adjoints (compact, like psiE / psiH)
   T* lpH[6];
-  double* grad;  // dJ/dK, summed over the three components
+  double* grad;  // dJ/dK per component: Ex cells, then Ey, then Ez
+  long long ncell;
   T idl[3];      // 1 / dl per axis
 };
 
@@ -86,7 +87,6 @@ __global__ void __launch_bounds__(256) k_adj_e(const __grid_constant__ StepArgs<
   T K[3];
   uint32_t w;
   cell_coeffs<T, CE, false>(a, nullptr, id, K, w);
-  double gsum = 0.0;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     // adj(E_c^{n+1}): identity part + the H update of step n+1 (forward
@@ -119,7 +119,8 @@ __global__ void __launch_bounds__(256) k_adj_e(const __grid_constant__ StepArgs<
       const long long qB = rB ? psi_index<T>(a.mape[axB], a.npe, axB, i, j, k, a.ny, a.nz) : -1;
       if (qA >= 0) g = add_rn(g, s.psiErec[2 * c][qA]);
       if (qB >= 0) g = sub_rn(g, s.psiErec[2 * c + 1][qB]);
-      gsum = __dadd_rn(gsum, __dmul_rn((double)x, (double)g));
+      const double gc = __dmul_rn((double)x, (double)g);
+      if (gc != 0.0) s.grad[c * s.ncell + id] = __dadd_rn(s.grad[c * s.ncell + id], gc);
       curl_transpose<T>(x, K[c], rA, rB, qA, qB, rA ? a.be[axA][pos[axA]] : T(0),
                         rA ? a.cpe[axA][pos[axA]] : T(0), rB ? a.be[axB][pos[axB]] : T(0),
                         rB ? a.cpe[axB][pos[axB]] : T(0), s.lpE[2 * c], s.lpE[2 * c + 1], qa,
@@ -129,7 +130,6 @@ __global__ void __launch_bounds__(256) k_adj_e(const __grid_constant__ StepArgs<
     s.gE[2 * c + 1][id] = qb;
     s.lamE[c][id] = x;
   }
-  if (gsum != 0.0) s.grad[id] = __dadd_rn(s.grad[id], gsum);
 }
 
 template <typename T>

@@ -190,13 +190,15 @@ def _smoothed_components(sim, dtype):
                                factor=sim.subpixel_factor, dtype=dtype)
 
 
-def build_tables(sim, dtype=None) -> dict:
+def build_tables(sim, dtype=None, ce3=None) -> dict:
     """Everything the engine consumes, in the forms the C ABI takes.
 
     dtype (np.float32 / np.float64) overrides the simulation's working
     precision: a float64 shadow of a float32 scene (the error statement of
     photonfdtd_b200.accuracy) evaluates every table as a float64 run of the
-    same scene would."""
+    same scene would. ``ce3`` (three grid-shaped arrays) replaces the E
+    coefficients of Ex, Ey, Ez outright (PF_CE_CELL3), as the reference's
+    value_and_grad_params does with its ce_of_params (jaxbackend.py:725-775)."""
     grid = sim.grid
     npdt = np.dtype(sim.dtypes["Ex"] if dtype is None else dtype).type
     dt, n_steps = float(sim.dt), int(sim.n_steps)
@@ -207,7 +209,8 @@ def build_tables(sim, dtype=None) -> dict:
                        for arr in (sim._b_e, sim._c_e, sim._b_h, sim._c_h)) for a in range(3)]
     edt = _eps_dtype(sim) if dtype is None else npdt
     custom = bool(getattr(sim, "_eps_r_custom", False))
-    need_ids = getattr(sim, "_has_dispersion", False) or not (custom or sim.subpixel)
+    need_ids = getattr(sim, "_has_dispersion", False) or not (custom or sim.subpixel
+                                                               or ce3 is not None)
     word = vals = med_ids = None
     media: list = []
     if need_ids:
@@ -215,7 +218,12 @@ def build_tables(sim, dtype=None) -> dict:
     ade = ade_tables(sim, med_ids, media, dt) if media else None
     if ade is not None and not ade["media"]:
         ade = None
-    if sim.subpixel and not custom:
+    if ce3 is not None:
+        if len(ce3) != 3 or any(np.shape(c) != tuple(grid.shape) for c in ce3):
+            raise ValueError("ce3 must hold three arrays of the grid's shape")
+        t["ce_mode"] = N.PF_CE_CELL3
+        t["ce"] = [np.ascontiguousarray(np.asarray(c), dtype=npdt) for c in ce3]
+    elif sim.subpixel and not custom:
         comps = _smoothed_components(sim, edt)
         t["ce_mode"] = N.PF_CE_CELL3
         t["ce"] = [np.ascontiguousarray((dt / (np.asarray(e) * EPS_0)).astype(edt, copy=False),
