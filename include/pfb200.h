@@ -204,6 +204,8 @@ int pf_set_state(pf_engine *eng, int64_t step, const void *src, int64_t bytes,
  *   pf_adj_add_field_source(step, comp, region, vals)
  *                               dJ/d(field snapshot taken after step `step`,
  *                               the FieldMonitor frame) over a strided region
+ *   pf_adj_set_flux_cotangent(mon, cot)
+ *                               dJ/d(flux integral) of flux monitor mon
  *   pf_adj_segment(step0, n, state)
  *                               for segments from the last to the first
  *                               (step0 + n must be where the reverse pass
@@ -216,6 +218,10 @@ int pf_set_state(pf_engine *eng, int64_t step, const void *src, int64_t bytes,
  * The engine's current state afterwards is the end of the last replay. */
 int pf_adj_init(pf_engine *eng, int64_t ring_steps);
 int pf_adj_set_dft_cotangent(pf_engine *eng, int mon, const double *cot);
+/* dJ/d(flux integral) of flux monitor mon: its plane's E and H enter the
+ * reverse pass as sources (the replay records the plane's tangential E per
+ * step for it). */
+int pf_adj_set_flux_cotangent(pf_engine *eng, int mon, double cot);
 int pf_adj_add_field_source(pf_engine *eng, int64_t step, int comp, const int32_t start[3],
                             const int32_t stop[3], const int32_t stride[3],
                             const double *vals);

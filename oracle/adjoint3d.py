@@ -25,14 +25,40 @@ import numpy as np
 from .fdtd_oracle import EPS0, OracleRun, _cls
 
 
+_PLANE = {0: ("Ey", "Ez", "Hy", "Hz"), 1: ("Ez", "Ex", "Hz", "Hx"), 2: ("Ex", "Ey", "Hx", "Hy")}
+
+
+def _flux_plane(run, m):
+    """(axis, index, dA) of a flux monitor, as OracleRun._flux takes them."""
+    g = run.grid
+    ax = {"x": 0, "y": 1, "z": 2}[m.plane_axis]
+    co = g.coords[ax]
+    i = 0 if co.size == 1 else int(np.argmin(np.abs(co - m.plane_position)))
+    w = [g.cell_size[a] if g.shape[a] > 1 else 1.0 for a in range(3)]
+    return ax, i, float(np.prod([w[a] for a in range(3) if a != ax]))
+
+
 class _RecordingRun(OracleRun):
     """An OracleRun that keeps, per step and E component, what the E
     coefficient multiplies: g = curl + sum(sign * psi') over the update's
-    region (psi' the slab's value after the step)."""
+    region (psi' the slab's value after the step), and per step each flux
+    monitor's plane of E_t1, E_t2, H_t1, H_t2 (t1 = axis+1, t2 = axis+2)."""
 
     def __init__(self, sim, n_steps=None, ce3=None):
         super().__init__(sim, n_steps, ce3=ce3)
         self.g_hist: List[Dict[str, np.ndarray]] = []
+        self.plane_hist: List[Dict[str, Tuple[np.ndarray, ...]]] = []
+
+    def _record(self, step):
+        planes = {}
+        for m in self.monitors:
+            if _cls(m) == "FluxMonitor":
+                ax, i, _ = _flux_plane(self, m)
+                sl = [slice(None)] * 3
+                sl[ax] = i
+                planes[m.name] = tuple(self.F[c][tuple(sl)].copy() for c in _PLANE[ax])
+        self.plane_hist.append(planes)
+        super()._record(step)
 
     def _apply(self, family):
         if family == "E":
@@ -110,11 +136,27 @@ def _reverse(sim, loss: Callable, ce3):
              for (_, _, _, _, slabs) in terms] for (_, _, _, _, _, terms) in run.updates]
     gk = {c: np.zeros(shape) for c in ("Ex", "Ey", "Ez")}
 
-    # the loss's sources per step: DFT samples and FieldMonitor frames
+    # the loss's sources per step: DFT samples, FieldMonitor frames and the
+    # flux integrand S = E_t1 H_t2 - E_t2 H_t1 summed over the plane (x dA dt)
     def sources(n):
         for m in run.monitors:
             kind = _cls(m)
-            if kind == "DFTMonitor":
+            if kind == "FluxMonitor":
+                G = out["flux"][m.name].grad
+                if G is None or float(G) == 0.0:
+                    continue
+                ax, i, da = _flux_plane(run, m)
+                c = float(G) * da * dt
+                e1, e2, h1, h2 = run.plane_hist[n][m.name]
+                n1, n2, m1, m2 = _PLANE[ax]
+                sl = [slice(None)] * 3
+                sl[ax] = i
+                sl = tuple(sl)
+                lam[n1][sl] += c * h2
+                lam[n2][sl] -= c * h1
+                lam[m2][sl] += c * e1
+                lam[m1][sl] -= c * e2
+            elif kind == "DFTMonitor":
                 st = run.dm[m.name]
                 if n not in st["steps"]:
                     continue

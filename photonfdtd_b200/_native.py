@@ -61,6 +61,7 @@ SIGNATURES = {
     "pf_step": (C.c_int, [_vp, _pi64]),
     "pf_adj_init": (C.c_int, [_vp, _i64]),
     "pf_adj_set_dft_cotangent": (C.c_int, [_vp, C.c_int, _pdbl]),
+    "pf_adj_set_flux_cotangent": (C.c_int, [_vp, C.c_int, _dbl]),
     "pf_adj_add_field_source": (C.c_int, [_vp, _i64, C.c_int, _pi32, _pi32, _pi32, _pdbl]),
     "pf_adj_segment": (C.c_int, [_vp, _i64, _i64, _vp, _i64, C.c_int]),
     "pf_adj_read_grad": (C.c_int, [_vp, _pdbl]),

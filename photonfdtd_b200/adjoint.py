@@ -16,9 +16,9 @@ The loss takes the reference's ``out`` dict with torch tensors instead of JAX
 arrays: ``{'fields': {name: {comp: (n_rec, *snap) real}}, 'dft': {name:
 {comp: (n_freq, *snap) complex128}}, 'flux': {name: scalar}}`` and returns a
 scalar tensor, e.g. ``lambda out: (out['dft']['d']['Ez'].abs() ** 2).sum()``.
-Flux is quadratic in the fields; a loss that depends on it raises
-NotImplementedError, as do dispersive media and subpixel smoothing (the
-reference raises for the latter two as well).
+Dispersive media raise NotImplementedError, as in the reference, and so
+does subpixel smoothing for value_and_grad_eps (value_and_grad_params takes
+per-component coefficients instead).
 """
 from __future__ import annotations
 
@@ -100,11 +100,12 @@ def _adjoint(sim, t: dict, loss: Callable, checkpoint_every) -> Tuple[float, np.
         eng._chk(eng._L.pf_adj_init(eng.h, every))
         if val.requires_grad:
             val.backward()
-        for name, v in out["flux"].items():
-            if v.grad is not None and float(v.grad) != 0.0:
-                raise NotImplementedError(
-                    f"the loss depends on flux monitor {name!r}; flux is quadratic in the "
-                    "fields and is not differentiated by the b200 adjoint")
+        # dJ/d(flux integrals): sources on each plane's E and H
+        for k, f in enumerate(t["flux"]):
+            v = out["flux"].get(f["m"].name)
+            if v is not None and v.grad is not None and float(v.grad) != 0.0:
+                eng._chk(eng._L.pf_adj_set_flux_cotangent(eng.h, eng.flux_ids[k],
+                                                          float(v.grad)))
         # dJ/d(DFT accumulators), per monitor in the engine's component order
         for k, d in enumerate(t["dft"]):
             m = d["m"]

@@ -58,6 +58,11 @@ struct FluxMon {
   int ring_cap = kRingMax;
   double* partial = nullptr;
   double* acc = nullptr;
+  // adjoint: dJ/dflux and the replay's E plane records (2 * n0 * n1 reals
+  // per recorded step, rec_cap steps)
+  double cot = 0.0;
+  void* rec = nullptr;
+  long long rec_cap = 0;
 };
 
 struct SrcFamily {
@@ -682,6 +687,15 @@ int record_step(pf_engine* e, long long t) {
     if (b) PF_CUDA(e, cudaMemcpyAsync(base + off, e->psiE[q], b, cudaMemcpyDeviceToDevice, e->stream));
     off += b;
   }
+  for (FluxMon& f : e->fluxes) {  // E planes of the flux monitors a loss depends on
+    if (f.cot == 0.0) continue;
+    if (t >= f.rec_cap) return fail(e, PF_ERR_STATE, "flux record slot out of range");
+    const long long np = (long long)f.p.n0 * f.p.n1;
+    k_flux_plane_record<T><<<(unsigned)((np + 255) / 256), 256, 0, e->stream>>>(
+        f.p, (const T*)e->E[e->cur][0], (const T*)e->E[e->cur][1], (const T*)e->E[e->cur][2],
+        (T*)f.rec + (size_t)t * 2 * np, e->ny, e->nz);
+  }
+  PF_CUDA(e, cudaGetLastError());
   return PF_OK;
 }
 
@@ -1401,7 +1415,7 @@ AdjState<T> adj_state(pf_engine* e, long long slot) {
 // The loss's sources on the fields sampled at step m, family fam (0: E^{m+1},
 // 1: H^{m+1/2}).
 template <typename T>
-int adj_sources(pf_engine* e, long long m, int fam) {
+int adj_sources(pf_engine* e, long long m, int fam, const AdjState<T>& st, long long slot) {
   const int B = 256;
   T* l[3];
   for (int c = 0; c < 3; ++c) l[c] = (T*)(fam == 0 ? e->lamE[c] : e->lamH[c]);
@@ -1413,6 +1427,13 @@ int adj_sources(pf_engine* e, long long m, int fam) {
     const long long nt = dm.r.ncell * dm.r.ncomp;
     k_adj_dft_src<T><<<(unsigned)((nt + B - 1) / B), B, 0, e->stream>>>(
         dm.r, e->dft_cot[k], ph, dm.n_freq, dm.dt, fam, l[0], l[1], l[2], e->ny, e->nz);
+  }
+  for (const FluxMon& f : e->fluxes) {
+    if (f.cot == 0.0) continue;
+    const long long np = (long long)f.p.n0 * f.p.n1;
+    k_adj_flux_src<T><<<(unsigned)((np + B - 1) / B), B, 0, e->stream>>>(
+        f.p, f.cot * f.dA * f.dt, fam, st.Hrec[0], st.Hrec[1], st.Hrec[2],
+        (const T*)f.rec + (size_t)slot * 2 * np, l[0], l[1], l[2], e->ny, e->nz);
   }
   for (const auto& rs : e->rsrc) {
     if (rs.step != m || (rs.comp >= 3) != (fam == 1)) continue;
@@ -1436,14 +1457,14 @@ int adj_segment_typed(pf_engine* e, long long step0, long long n) {
   const StepArgs<T> a = step_args<T>(e);
   for (long long m = step0 + n - 1; m >= step0; --m) {
     const AdjState<T> s = adj_state<T>(e, m - step0);
-    if ((rc = adj_sources<T>(e, m, 0))) return rc;
+    if ((rc = adj_sources<T>(e, m, 0, s, m - step0))) return rc;
     if (e->ce_mode == PF_CE_CELL1)
       k_adj_e<T, kCeCell1><<<grd, blk, 0, e->stream>>>(a, s);
     else if (e->ce_mode == PF_CE_CELL3)
       k_adj_e<T, kCeCell3><<<grd, blk, 0, e->stream>>>(a, s);
     else
       k_adj_e<T, kCeTable><<<grd, blk, 0, e->stream>>>(a, s);
-    if ((rc = adj_sources<T>(e, m, 1))) return rc;
+    if ((rc = adj_sources<T>(e, m, 1, s, m - step0))) return rc;
     k_adj_h<T><<<grd, blk, 0, e->stream>>>(a, s);
   }
   PF_CUDA(e, cudaGetLastError());
@@ -1535,6 +1556,22 @@ int pf_adj_set_dft_cotangent(pf_engine* e, int mon, const double* cot) {
   if (!e->dft_cot[mon] && (rc = dalloc(e, (void**)&e->dft_cot[mon], bytes))) return rc;
   PF_CUDA(e, cudaMemcpyAsync(e->dft_cot[mon], cot, bytes, cudaMemcpyHostToDevice, e->stream));
   PF_CUDA(e, cudaStreamSynchronize(e->stream));
+  return PF_OK;
+}
+
+int pf_adj_set_flux_cotangent(pf_engine* e, int mon, double cot) {
+  if (!e) return PF_ERR_INVALID;
+  if (!e->adj) return fail(e, PF_ERR_STATE, "pf_adj_set_flux_cotangent before pf_adj_init");
+  if (mon < 0 || mon >= (int)e->fluxes.size()) return fail(e, PF_ERR_INVALID, "bad flux monitor");
+  if (!std::isfinite(cot)) return fail(e, PF_ERR_INVALID, "flux cotangent must be finite");
+  FluxMon& f = e->fluxes[mon];
+  if (cot != 0.0 && f.rec_cap < e->ring_steps) {
+    int rc;
+    const size_t bytes = (size_t)e->ring_steps * 2 * f.p.n0 * f.p.n1 * e->rb;
+    if ((rc = dalloc(e, &f.rec, bytes))) return rc;
+    f.rec_cap = e->ring_steps;
+  }
+  f.cot = cot;
   return PF_OK;
 }
 

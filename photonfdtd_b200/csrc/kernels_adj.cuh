@@ -25,6 +25,7 @@
 #pragma once
 
 #include "cell_update.cuh"
+#include "kernels_aux.cuh"
 
 namespace pfb {
 
@@ -223,6 +224,56 @@ __global__ void k_adj_region_src(DftRegion r, const double* vals, T* l, int ny, 
                         (r.start[1] + cj * r.stride[1])) * nz +
                        (r.start[2] + ck * r.stride[2]);
   l[id] = to_real(__dadd_rn((double)l[id], vals[cell]), T());
+}
+
+// ---- flux losses ----------------------------------------------------------
+// A flux monitor adds S dA dt per step, S = E_t1 H_t2 - E_t2 H_t1 summed over
+// its plane (E at n+1, H at n+1/2; t1, t2 the tangential axes in cyclic
+// order, as k_flux_sample_batch). With c = dJ/dflux * dA * dt its sources on
+// the adjoint are dS/dE_t1 = H_t2, dS/dE_t2 = -H_t1, dS/dH_t2 = E_t1,
+// dS/dH_t1 = -E_t2 at every plane cell.
+__device__ __forceinline__ long long flux_cell(const FluxPlane& p, long long t, int ny, int nz) {
+  const int u = (int)(t / p.n1), w = (int)(t % p.n1);
+  if (p.axis == 0) return ((long long)p.idx * ny + u) * nz + w;
+  if (p.axis == 1) return ((long long)u * ny + p.idx) * nz + w;
+  return ((long long)u * ny + w) * nz + p.idx;
+}
+
+// E_t1, E_t2 of the plane after a step, into a record of 2 * n0 * n1 reals.
+template <typename T>
+__global__ void k_flux_plane_record(FluxPlane p, const T* E0, const T* E1, const T* E2, T* dst,
+                                    int ny, int nz) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long np = (long long)p.n0 * p.n1;
+  if (t >= np) return;
+  const long long id = flux_cell(p, t, ny, nz);
+  const T* E[3] = {E0, E1, E2};
+  dst[t] = E[(p.axis + 1) % 3][id];
+  dst[np + t] = E[(p.axis + 2) % 3][id];
+}
+
+// fam 0: lamE_t1 += c H_t2, lamE_t2 -= c H_t1 from the recorded H (full
+// fields); fam 1: lamH_t2 += c E_t1, lamH_t1 -= c E_t2 from the plane record.
+template <typename T>
+__global__ void k_adj_flux_src(FluxPlane p, double c, int fam, const T* H0, const T* H1,
+                               const T* H2, const T* erec, T* l0, T* l1, T* l2, int ny, int nz) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long np = (long long)p.n0 * p.n1;
+  if (t >= np) return;
+  const long long id = flux_cell(p, t, ny, nz);
+  const int t1 = (p.axis + 1) % 3, t2 = (p.axis + 2) % 3;
+  T* l[3] = {l0, l1, l2};
+  double a, b;  // sources on component t1, t2
+  if (fam == 0) {
+    const T* H[3] = {H0, H1, H2};
+    a = c * (double)H[t2][id];
+    b = -c * (double)H[t1][id];
+  } else {
+    b = c * (double)erec[t];        // on H_t2
+    a = -c * (double)erec[np + t];  // on H_t1
+  }
+  l[t1][id] = to_real(__dadd_rn((double)l[t1][id], a), T());
+  l[t2][id] = to_real(__dadd_rn((double)l[t2][id], b), T());
 }
 
 }  // namespace pfb

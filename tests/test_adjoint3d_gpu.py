@@ -3,7 +3,8 @@ counterpart of jaxbackend.py:666-722) against central finite differences of
 the forward engine in float64: a 3D scene with CPML on every face, a
 dielectric cube, an Ey dipole, a DFT plane (E and H components) and a
 downsampled FieldMonitor frame, J mixing |DFT|^2, a cross term and frame
-terms; and a 2D TM scene (z collapsed). Every term of J is scaled by its
+terms; the same scene with flux planes across x and y in J (linear and
+squared flux); and a 2D TM scene (z collapsed). Every term of J is scaled by its
 value on the unperturbed scene so that each one counts. Each checked cell's
 gradient must agree with (J(eps + h) - J(eps - h)) / 2h to 1e-6 of the
 largest gradient magnitude; the whole gradient must match the oracle's
@@ -59,6 +60,17 @@ TERMS3D = [lambda o: (o["dft"]["d"]["Ey"].abs() ** 2).sum(),
            lambda o: (o["dft"]["d"]["Hx"].real * o["dft"]["d"]["Ey"].imag).sum(),
            lambda o: (o["fields"]["f"]["Ex"] ** 2).sum(),
            lambda o: o["fields"]["f"]["Hz"].sum()]
+def scene3d_flux(precision="float64", eps=None):
+    """scene3d with flux planes across x and y in the loss."""
+    sim = scene3d(precision, eps)
+    sim.add_monitor(pf.FluxMonitor(name="fx", plane_axis="x", plane_position=0.4e-6))
+    sim.add_monitor(pf.FluxMonitor(name="fy", plane_axis="y", plane_position=-0.16e-6))
+    return sim
+
+
+TERMS3D_FLUX = [lambda o: (o["dft"]["d"]["Ey"].abs() ** 2).sum(),
+                lambda o: o["flux"]["fx"],
+                lambda o: o["flux"]["fy"] ** 2]
 TERMS2D = [lambda o: (o["dft"]["d"]["Ez"].abs() ** 2).sum(),
            lambda o: (o["dft"]["d"]["Hy"].real * o["dft"]["d"]["Ez"].imag).sum()]
 
@@ -111,6 +123,10 @@ def test_adjoint2d_tm_matches_central_differences():
     check_fd(scene2d, TERMS2D, 10, 4)
 
 
+def test_flux_loss_matches_central_differences():
+    check_fd(scene3d_flux, TERMS3D_FLUX, 10, 6)
+
+
 def test_checkpoint_spacing_does_not_change_the_gradient():
     loss = scaled_loss(scene3d, TERMS3D)
     _, g1 = value_and_grad_eps(scene3d(), loss)
@@ -135,13 +151,10 @@ def test_unsupported_cases_raise():
     sim.subpixel = True
     with pytest.raises(NotImplementedError):
         value_and_grad_eps(sim, loss)
-    sim = scene3d()
-    sim.add_monitor(pf.FluxMonitor(name="fx", plane_axis="x", plane_position=0.4e-6))
-    with pytest.raises(NotImplementedError):
-        value_and_grad_eps(sim, lambda o: loss(o) + o["flux"]["fx"])
 
 
-@pytest.mark.parametrize("build,terms", [(scene3d, TERMS3D), (scene2d, TERMS2D)])
+@pytest.mark.parametrize("build,terms", [(scene3d, TERMS3D), (scene2d, TERMS2D),
+                                         (scene3d_flux, TERMS3D_FLUX)])
 def test_engine_adjoint_matches_oracle_adjoint(build, terms):
     """The engine's per-cell adjoint kernels against the oracle's transposed
     slab step (oracle/adjoint3d.py), both float64: the values agree to the

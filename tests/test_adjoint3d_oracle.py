@@ -2,7 +2,8 @@
 jaxbackend.py:666-722's jax.grad computes) against central differences of
 the oracle's own forward run, float64, on tiny scenes: a 3D grid with CPML
 on every face (DFT plane with E and H components, a downsampled FieldMonitor
-frame) and a 2D TM grid. Pins the transposed step before the engine's adjoint
+frame; the same with flux planes across x and z in the loss) and a 2D TM
+grid. Pins the transposed step before the engine's adjoint
 is compared with it on the GPU."""
 import numpy as np
 import pytest
@@ -51,6 +52,20 @@ def loss3d_terms():
             lambda o: (o["fields"]["f"]["Ey"] ** 2).sum()]
 
 
+def tiny3d_flux(eps=None):
+    """tiny3d with flux planes across x and z."""
+    sim = tiny3d(eps)
+    sim.add_monitor(pf.FluxMonitor(name="fx", plane_axis="x", plane_position=0.24e-6))
+    sim.add_monitor(pf.FluxMonitor(name="fz", plane_axis="z", plane_position=-0.08e-6))
+    return sim
+
+
+def loss3d_flux_terms():
+    return [lambda o: (o["dft"]["d"]["Ez"].abs() ** 2).sum(),
+            lambda o: o["flux"]["fx"],
+            lambda o: o["flux"]["fz"] ** 2]
+
+
 def loss2d_terms():
     return [lambda o: (o["dft"]["d"]["Ez"].abs() ** 2).sum(),
             lambda o: (o["dft"]["d"]["Hx"].abs() ** 2).sum()]
@@ -66,7 +81,8 @@ def scaled(build, terms):
     return lambda o: sum(w * t(o) for w, t in zip(s, terms))
 
 
-@pytest.mark.parametrize("build,terms,seed", [(tiny3d, loss3d_terms, 1), (tiny2d, loss2d_terms, 2)])
+@pytest.mark.parametrize("build,terms,seed", [(tiny3d, loss3d_terms, 1), (tiny2d, loss2d_terms, 2),
+                                               (tiny3d_flux, loss3d_flux_terms, 5)])
 def test_oracle_gradient_matches_central_differences(build, terms, seed):
     loss = scaled(build, terms())
     sim = build()
