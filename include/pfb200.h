@@ -101,6 +101,19 @@ int pf_set_ade(pf_engine *eng, int n_media, const int64_t *count,
                const int32_t *npole, const double *coef, const double *inv_eps,
                const double *ce_m, const uint32_t *cell_word);
 
+/* Host-side helper for the ADE cell words, no engine needed: `word` holds,
+ * per cell in C order, either a plain entry (bit 31 clear: a table index, or
+ * anything when clear_plain != 0) or a dispersive entry bit 31 | m << 27
+ * with its low 27 bits zero (m < n_media). Each dispersive entry receives
+ * its rank among medium m's cells in C order (the record index
+ * pf_set_ade's words carry), counts[m] the number of medium m's cells;
+ * clear_plain != 0 zeroes every plain entry (the cell_word of the per-cell
+ * coefficient modes). One pass, in place. This is the compact dispersive
+ * cell numbering of src/photonfdtd/simulation.py:592-636. Errors go to
+ * pf_last_error(NULL). */
+int pf_rank_dispersive_words(uint32_t *word, int64_t n, int n_media, int64_t *counts,
+                             int clear_plain);
+
 /* Soft point sources (simulation.py:1367-1390; rustbackend.py:151-166).
  * n_src entries in the reference's source order: comp (0..5), flat cell
  * index i*ny*nz + j*nz + k, waveform row, amplitude. wave = n_wave rows of

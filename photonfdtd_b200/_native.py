@@ -48,6 +48,7 @@ SIGNATURES = {
     "pf_set_ce": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _pu32, C.c_int, _pdbl]),
     "pf_set_cpml": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp]),
     "pf_set_ade": (C.c_int, [_vp, C.c_int, _pi64, _pi32, _pdbl, _pdbl, _pdbl, _pu32]),
+    "pf_rank_dispersive_words": (C.c_int, [_pu32, _i64, C.c_int, _pi64, C.c_int]),
     "pf_set_sources": (C.c_int, [_vp, C.c_int, _pi32, _pi64, _pi32, _pdbl, C.c_int, _pdbl]),
     "pf_add_dft": (C.c_int, [_vp, _pi32, _pi32, _pi32, C.c_int, C.c_int, C.c_int, _pdbl, _pdbl,
                              _dbl, C.POINTER(C.c_int)]),

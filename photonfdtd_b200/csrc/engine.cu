@@ -931,6 +931,31 @@ int pf_set_ade(pf_engine* e, int n_media, const int64_t* count, const int32_t* n
   return PF_OK;
 }
 
+int pf_rank_dispersive_words(uint32_t* word, int64_t n, int n_media, int64_t* counts,
+                             int clear_plain) {
+  if (!word || !counts || n < 0) return fail(nullptr, PF_ERR_INVALID, "NULL word or counts");
+  if (n_media < 0 || n_media > kMaxMedia)
+    return fail(nullptr, PF_ERR_UNSUPPORTED, "at most %d dispersive media, got %d", kMaxMedia,
+                n_media);
+  long long cnt[kMaxMedia] = {0};
+  for (long long q = 0; q < n; ++q) {
+    const uint32_t w = word[q];
+    if (!(w & kDispersiveBit)) {
+      if (clear_plain) word[q] = 0u;
+      continue;
+    }
+    const int m = (int)((w >> kMediumShift) & 15u);
+    if (m >= n_media || (w & kLocMask))
+      return fail(nullptr, PF_ERR_INVALID, "bad dispersive word 0x%08x at cell %lld", w, q);
+    if (cnt[m] > (long long)kLocMask)
+      return fail(nullptr, PF_ERR_UNSUPPORTED, "more than 2^%d cells in one dispersive medium",
+                  kMediumShift);
+    word[q] = w | (uint32_t)cnt[m]++;
+  }
+  for (int m = 0; m < n_media; ++m) counts[m] = cnt[m];
+  return PF_OK;
+}
+
 int pf_set_sources(pf_engine* e, int n_src, const int32_t* comp, const int64_t* cell,
                    const int32_t* wave_row, const double* amp, int n_wave, const double* wave) {
   if (!e) return PF_ERR_INVALID;

@@ -14,6 +14,8 @@ from __future__ import annotations
 
 from typing import Dict, List, Optional, Tuple
 
+import ctypes
+
 import numpy as np
 
 from . import _native as N
@@ -59,6 +61,15 @@ def _cells(structure, grid):
     return structure.region_mask(grid)
 
 
+def _stamp(arr, sel, value) -> None:
+    """arr[sel] = value; a boolean mask goes through copyto(where=), which
+    numpy runs about twice as fast as masked assignment."""
+    if isinstance(sel, np.ndarray) and sel.dtype == np.bool_:
+        np.copyto(arr, arr.dtype.type(value), where=sel)
+    else:
+        arr[sel] = value
+
+
 def _medium_eps(med) -> float:
     return float(med.eps_r)
 
@@ -67,7 +78,10 @@ def _eps_dtype(sim):
     return np.dtype(sim.dtypes["eps_r"]).type
 
 
-def material_words(sim, edt=None):
+_MAX_MEDIA = 16  # dispersive media one engine takes (4 bits of the ADE word)
+
+
+def material_words(sim, edt=None, disp_bits=False):
     """Per-cell uint32 word in table mode, the table values, and ADE cells.
 
     Stamps value indices instead of permittivities in structure order
@@ -75,13 +89,16 @@ def material_words(sim, edt=None):
     the dispersive medium id (simulation.py:579-590). Returns
     (word, eps_values, med_ids, media) where med_ids is an int16 grid
     (-1 = not dispersive) and media the dispersive media in first-use order.
+    With ``disp_bits`` a dispersive structure stamps 0x80000000 | m << 27
+    (m its medium's first-use index) in place of a value index and med_ids
+    is None: pf_rank_dispersive_words then numbers each medium's cells.
     """
     grid = sim.grid
     shape = tuple(grid.shape)
     vals: List[float] = [1.0]
     lookup: Dict[float, int] = {1.0: 0}
     word = np.zeros(shape, dtype=np.uint32)
-    med_ids = np.full(shape, -1, dtype=np.int16)
+    med_ids = None if disp_bits else np.full(shape, -1, dtype=np.int16)
     media, med_index = [], {}
     edt = _eps_dtype(sim) if edt is None else edt
     for s in sim.structures:
@@ -93,21 +110,31 @@ def material_words(sim, edt=None):
         if v not in lookup:
             lookup[v] = len(vals)
             vals.append(v)
-        word[sel] = lookup[v]
-        if getattr(med, "is_dispersive", False):
-            if id(med) not in med_index:
-                med_index[id(med)] = len(media)
-                media.append(med)
-            med_ids[sel] = med_index[id(med)]
-        else:
-            med_ids[sel] = -1
+        disp = getattr(med, "is_dispersive", False)
+        if disp and id(med) not in med_index:
+            med_index[id(med)] = len(media)
+            media.append(med)
+        if disp_bits:
+            if disp:
+                m = med_index[id(med)]
+                if m >= _MAX_MEDIA:
+                    raise NotImplementedError(
+                        f"at most {_MAX_MEDIA} dispersive media, the scene has more")
+                _stamp(word, sel, 0x80000000 | (m << 27))
+            else:
+                _stamp(word, sel, lookup[v])
+            continue
+        _stamp(word, sel, lookup[v])
+        _stamp(med_ids, sel, med_index[id(med)] if disp else -1)
     return word, np.array(vals, dtype=edt), med_ids, media
 
 
-def ade_tables(sim, med_ids, media, dt):
+def ade_tables(sim, med_ids, media, dt, counts=None):
     """Compact dispersive-cell indexing and pole coefficients
     (simulation.py:592-636): a = (2 - w0^2 dt^2)/(1 + g dt),
-    b = (g dt - 1)/(1 + g dt), c = eps0 S dt^2/(1 + g dt), per pole."""
+    b = (g dt - 1)/(1 + g dt), c = eps0 S dt^2/(1 + g dt), per pole.
+    ``counts`` (cells per medium, from pf_rank_dispersive_words) replaces
+    the scan of med_ids: every medium is kept, cell lists are not built."""
     wmax = 0.0
     for med in media:
         wmax = max(wmax, med.max_pole_omega() * dt)
@@ -117,16 +144,19 @@ def ade_tables(sim, med_ids, media, dt):
             "makes the explicit ADE update unstable at this resolution. Use a finer "
             "grid, restrict the medium to poles inside the simulation band, or use "
             "DispersiveMedium.at_wavelength(lambda) for a fixed-index Medium.")
-    flat = med_ids.ravel()
+    flat = None if counts is not None else med_ids.ravel()
     kept, base, count, npole, coef, inv, cells = [], [], [], [], [], [], []
     g = 0
     for m, med in enumerate(media):
-        idx = np.flatnonzero(flat == m)
-        if idx.size == 0:
-            continue
+        n = int(counts[m]) if counts is not None else None
+        idx = np.flatnonzero(flat == m) if counts is None else None
+        if counts is None:
+            if idx.size == 0:
+                continue
+            n = idx.size
         kept.append(med)
         base.append(g)
-        count.append(idx.size)
+        count.append(n)
         npole.append(len(med.poles))
         for p in med.poles:
             den = 1.0 + p.gamma * dt
@@ -134,7 +164,7 @@ def ade_tables(sim, med_ids, media, dt):
                      (EPS_0 * p.strength * dt ** 2) / den]
         inv.append(1.0 / (EPS_0 * med.eps_inf))
         cells.append(idx)
-        g += idx.size
+        g += n
     return dict(media=kept, base=np.array(base, np.int64), count=np.array(count, np.int64),
                 npole=np.array(npole, np.int32), coef=np.array(coef, np.float64),
                 inv=np.array(inv, np.float64), cells=cells)
@@ -211,13 +241,24 @@ def build_tables(sim, dtype=None, ce3=None) -> dict:
     custom = bool(getattr(sim, "_eps_r_custom", False))
     need_ids = getattr(sim, "_has_dispersion", False) or not (custom or sim.subpixel
                                                                or ce3 is not None)
-    word = vals = med_ids = None
+    word = vals = None
     media: list = []
     if need_ids:
-        word, vals, med_ids, media = material_words(sim, edt)
-    ade = ade_tables(sim, med_ids, media, dt) if media else None
-    if ade is not None and not ade["media"]:
-        ade = None
+        word, vals, _, media = material_words(sim, edt, disp_bits=True)
+    table_mode = ce3 is None and not (sim.subpixel and not custom) and not custom
+    ade = None
+    if media:
+        # rank the dispersive cells per medium in one native pass: in place in
+        # table mode (the ce word carries them), else in a copy whose plain
+        # cells are zeroed (the separate ADE cell word)
+        cw = word.reshape(-1) if table_mode else word.reshape(-1).copy()
+        counts = np.zeros(len(media), np.int64)
+        N.check(N.lib().pf_rank_dispersive_words(N.ptr(cw, ctypes.c_uint32), cw.size, len(media),
+                                                 N.ptr(counts, ctypes.c_int64),
+                                                 0 if table_mode else 1))
+        if counts.sum() > 0:
+            ade = ade_tables(sim, None, media, dt, counts=counts)
+            ade["cell_word"] = None if table_mode else cw
     if ce3 is not None:
         if len(ce3) != 3 or any(np.shape(c) != tuple(grid.shape) for c in ce3):
             raise ValueError("ce3 must hold three arrays of the grid's shape")
@@ -239,25 +280,10 @@ def build_tables(sim, dtype=None, ce3=None) -> dict:
         t["word"] = word
     if ade is not None:
         # dispersive word: bit 31 | medium << 27 | rank of the cell among the
-        # medium's cells in C order
-        if any(c > (1 << 27) for c in ade["count"]):
-            raise NotImplementedError("more than 2^27 cells in one dispersive medium")
-        flat_word = np.zeros(int(np.prod(grid.shape)), dtype=np.uint32)
-        ce_m = []
-        for m, med in enumerate(ade["media"]):
-            cells = ade["cells"][m]
-            flat_word[cells] = (np.uint32(0x80000000) | np.uint32(m << 27)
-                                | np.arange(cells.size, dtype=np.uint32))
-            # the coefficient a dispersive cell gets from its stamped eps_inf
-            ce_m.append(float((dt / (np.array([med.eps_r], dtype=edt) * EPS_0)).astype(edt)[0]))
-        ade["ce_m"] = np.array(ce_m, np.float64)
-        if t["ce_mode"] == N.PF_CE_TABLE:
-            w = t["word"].ravel()
-            for m in range(len(ade["media"])):
-                w[ade["cells"][m]] = flat_word[ade["cells"][m]]
-            ade["cell_word"] = None
-        else:
-            ade["cell_word"] = flat_word
+        # medium's cells in C order (pf_rank_dispersive_words above); the
+        # coefficient a dispersive cell gets from its stamped eps_inf
+        ade["ce_m"] = np.array([float((dt / (np.array([med.eps_r], dtype=edt) * EPS_0))
+                                      .astype(edt)[0]) for med in ade["media"]], np.float64)
         del ade["cells"]
     t["ade"] = ade
     t["sources"] = source_tables(sim, n_steps, dt)

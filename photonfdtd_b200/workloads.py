@@ -130,8 +130,13 @@ class BlockMedium:
 
     def region_mask(self, grid) -> np.ndarray:
         b = self._block
-        m = (self._ids == self._which).repeat(b, 0).repeat(b, 1).repeat(b, 2)
+        sel = self._ids == self._which
+        n0, n1, n2 = sel.shape
+        m = np.broadcast_to(sel[:, None, :, None, :, None],
+                            (n0, b, n1, b, n2, b)).reshape(n0 * b, n1 * b, n2 * b)
         shape = tuple(grid.shape)
+        if m.shape == shape:
+            return m
         out = np.zeros(shape, dtype=bool)
         n = [min(shape[a], m.shape[a]) for a in range(3)]
         out[:n[0], :n[1], :n[2]] = m[:n[0], :n[1], :n[2]]
