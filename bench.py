@@ -386,9 +386,10 @@ def e2e_bench(size: int, steps: int, world: int, dist) -> dict:
         sim = W.config3(pf, n_total=size, n_steps=steps, union_blocks=True)
         api = "photonfdtd_b200.Simulation(...).run()"
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    res = sim.run()
-    wall = time.perf_counter() - t0
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        t0 = time.perf_counter()
+        res = sim.run()
+        wall = time.perf_counter() - t0
     st = dict(E.LAST_RUN)
     if not (len(res.flux) == 6 and "d" in res.dft and np.isfinite(list(res.flux.values())).all()):
         raise RuntimeError("e2e: Simulation.run() returned an incomplete Result")
@@ -400,6 +401,7 @@ def e2e_bench(size: int, steps: int, world: int, dist) -> dict:
             "phases_s": {"tables": round(st["tables_s"], 3), "engine": round(st["create_s"], 3),
                          "steps": round(st["advance_s"], 3),
                          "steps_and_readback": round(st["run_s"], 3)},
+            "clocks": clk.summary(),
             "what": f"{api}: config 3 at {size}^3 for {steps} steps, host scene in, "
                     "Result (DFT + flux) out, wall clock"}
 
