@@ -17,6 +17,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -93,7 +95,9 @@ struct pf_engine {
   // staged tables
   int ce_mode = -1;
   std::vector<char> h_ce[3];
-  std::vector<uint32_t> h_word;
+  // PF_CE_TABLE: the word goes to the device in pf_set_ce; word_need[m] is
+  // 1 + the largest record index its dispersive words give medium m (0: none)
+  long long word_need[kMaxMedia] = {};
   std::vector<double> h_table;
   std::vector<char> h_cpml[3][4];  // b_e, c_e, b_h, c_h
   int n_media = 0;
@@ -228,8 +232,25 @@ int upload(pf_engine* e, void** p, const void* src, size_t bytes) {
 // significand a in [1, 2). Sign and binade of a do not change the outcome
 // while nothing over- or underflows; the device's 2^64 prescaling and the
 // range check on d below keep every input of the fast path in that regime.
-// About 8.4M fmaf evaluations (~50 ms).
+// About 8.4M fmaf evaluations (~50 ms); the answer per divisor is kept for
+// the process, so engines on the same grid spacing check it once.
+bool recip_division_exact_scan(float d);
 bool recip_division_exact(float d) {
+  static std::mutex mu;
+  static std::map<uint32_t, bool> known;
+  uint32_t key;
+  memcpy(&key, &d, 4);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = known.find(key);
+    if (it != known.end()) return it->second;
+  }
+  const bool ok = recip_division_exact_scan(d);
+  std::lock_guard<std::mutex> lk(mu);
+  known[key] = ok;
+  return ok;
+}
+bool recip_division_exact_scan(float d) {
   if (!(d >= 0x1p-30f && d <= 0x1p-23f)) return false;
   const float r = 1.0f / d;
   for (uint32_t m = 0; m < (1u << 23); ++m) {
@@ -353,7 +374,6 @@ int finalize_typed(pf_engine* e) {
     for (int c = 0; c < 3; ++c)
       if ((rc = upload(e, &e->ce[c], e->h_ce[c].data(), n * S))) return rc;
   } else {
-    if ((rc = upload(e, (void**)&e->word, e->h_word.data(), n * 4))) return rc;
     std::vector<T> tab(e->h_table.size());
     for (size_t q = 0; q < tab.size(); ++q) tab[q] = (T)e->h_table[q];
     if ((rc = upload(e, &e->table, tab.data(), tab.size() * S))) return rc;
@@ -858,7 +878,6 @@ int pf_set_ce(pf_engine* e, int mode, const void* ce0, const void* ce1, const vo
   if (e->finalized) return fail(e, PF_ERR_STATE, "pf_set_ce after pf_finalize");
   const size_t bytes = (size_t)e->ncell * e->rb;
   for (int c = 0; c < 3; ++c) e->h_ce[c].clear();
-  e->h_word.clear();
   e->h_table.clear();
   if (mode == PF_CE_CELL1) {
     if (!ce0) return fail(e, PF_ERR_INVALID, "PF_CE_CELL1 needs ce0");
@@ -869,10 +888,29 @@ int pf_set_ce(pf_engine* e, int mode, const void* ce0, const void* ce1, const vo
     for (int c = 0; c < 3; ++c) e->h_ce[c].assign((const char*)src[c], (const char*)src[c] + bytes);
   } else if (mode == PF_CE_TABLE) {
     if (!word || n_table < 1 || !table) return fail(e, PF_ERR_INVALID, "PF_CE_TABLE needs word and table");
-    for (long long q = 0; q < e->ncell; ++q)
-      if (!(word[q] & kDispersiveBit) && word[q] >= (uint32_t)n_table)
-        return fail(e, PF_ERR_INVALID, "ce word %u at cell %lld exceeds table size %d", word[q], q, n_table);
-    e->h_word.assign(word, word + e->ncell);
+    // one pass: plain words index the table; per medium, the largest record
+    // index its dispersive words name (checked against its cell count at
+    // pf_finalize). The word then goes to the device straight from the
+    // caller's buffer, with no host copy.
+    long long need[kMaxMedia] = {};
+    for (long long q = 0; q < e->ncell; ++q) {
+      const uint32_t w = word[q];
+      if (w & kDispersiveBit) {
+        const int m = (int)((w >> kMediumShift) & 15u);
+        need[m] = std::max(need[m], (long long)(w & kLocMask) + 1);
+      } else if (w >= (uint32_t)n_table) {
+        return fail(e, PF_ERR_INVALID, "ce word %u at cell %lld exceeds table size %d", w, q, n_table);
+      }
+    }
+    const size_t wb = (size_t)e->ncell * 4;
+    PF_CUDA(e, cudaSetDevice(e->device));
+    if (!e->word) {
+      int rc = dalloc(e, (void**)&e->word, wb);
+      if (rc) return rc;
+    }
+    PF_CUDA(e, cudaMemcpyAsync(e->word, word, wb, cudaMemcpyHostToDevice, e->stream));
+    PF_CUDA(e, cudaStreamSynchronize(e->stream));
+    memcpy(e->word_need, need, sizeof need);
     e->h_table.assign(table, table + n_table);
   } else {
     return fail(e, PF_ERR_INVALID, "unknown ce mode %d", mode);
@@ -1061,13 +1099,11 @@ int pf_finalize(pf_engine* e) {
   if (e->n_media > 0 && e->ce_mode == PF_CE_CELL1 && e->h_adeword.size() != (size_t)e->ncell)
     return fail(e, PF_ERR_INVALID, "PF_CE_CELL1 with dispersive media needs cell_word");
   if (e->ce_mode == PF_CE_TABLE)
-    for (long long q = 0; q < e->ncell; ++q) {
-      const uint32_t w = e->h_word[q];
-      if (!(w & kDispersiveBit)) continue;
-      const uint32_t m = (w >> kMediumShift) & 15u;
-      if ((int)m >= e->n_media || (long long)(w & kLocMask) >= e->m_count[m])
-        return fail(e, PF_ERR_INVALID, "bad dispersive word 0x%08x at cell %lld", w, q);
-    }
+    for (int m = 0; m < kMaxMedia; ++m)
+      if (e->word_need[m] > 0 && (m >= e->n_media || e->word_need[m] > e->m_count[m]))
+        return fail(e, PF_ERR_INVALID,
+                    "bad dispersive word: medium %d record %lld, but the medium has %lld cells", m,
+                    e->word_need[m] - 1, m < e->n_media ? e->m_count[m] : 0LL);
   const bool has_h_src = !e->src[1].cell.empty();
   const bool fusable = fused_supported(e->nx, e->ny, e->nz) && !has_h_src;
   if (e->kernel == PF_KERNEL_FUSED && !fusable)
@@ -1120,7 +1156,6 @@ int pf_finalize(pf_engine* e) {
   }
   // host staging no longer needed
   for (int c = 0; c < 3; ++c) std::vector<char>().swap(e->h_ce[c]);
-  std::vector<uint32_t>().swap(e->h_word);
   std::vector<uint32_t>().swap(e->h_adeword);
   e->finalized = true;
   return PF_OK;
