@@ -76,7 +76,10 @@ int pf_create(int nx, int ny, int nz, int real_bytes, double dx, double dy,
  *  PF_CE_TABLE: word = nx*ny*nz uint32; word w < 2^31 selects table[w] (the
  *    word must be < n_table); w >= 2^31 marks a dispersive cell whose
  *    coefficient comes from its medium (pf_set_ade). table = n_table reals
- *    given as doubles (each exactly representable in the real type). */
+ *    given as doubles (each exactly representable in the real type). The
+ *    word is checked and copied to device memory during the call (one pass
+ *    over it, no host copy); its dispersive words are checked against the
+ *    media's cell counts at pf_finalize. */
 int pf_set_ce(pf_engine *eng, int mode, const void *ce0, const void *ce1,
               const void *ce2, const uint32_t *word, int n_table,
               const double *table);
