@@ -5,7 +5,8 @@ dispersive cell carries bit 31 | medium << 27 | its rank among that medium's
 cells in C order. Checked on the config-3 block scene (table mode), on a
 scene whose first dispersive medium is painted over completely (it keeps its
 slot with zero cells), and on a custom-eps scene (per-cell coefficient mode,
-separate ADE word with plain cells zero); plus the helper's own errors."""
+separate ADE word with plain cells zero); plus the helper's own errors.
+On the GPU, the painted-over scene runs bit for bit against the oracle."""
 import ctypes
 
 import numpy as np
@@ -52,7 +53,7 @@ def test_config3_table_words():
     assert t["ade"]["cell_word"] is None
 
 
-def painted_over(custom=False):
+def painted_over(custom=False, precision="float64", monitors=()):
     grid = pf.Grid(size=(0.64e-6, 0.48e-6, 0.4e-6), cell_size=40e-9, pml_layers=2)
     boxes = [pf.Box(center=(0.0, 0.0, 0.0), size=(0.2e-6, 0.2e-6, 0.2e-6), medium=drude()),
              pf.Box(center=(0.0, 0.0, 0.0), size=(0.3e-6, 0.3e-6, 0.3e-6),
@@ -61,7 +62,8 @@ def painted_over(custom=False):
                     medium=lorentz())]
     src = pf.PointDipole(position=(-0.2e-6, 0.0, 0.0), component="Ez",
                          waveform=pf.GaussianPulse(freq0=C_0 / 1e-6, fwhm=4e-15))
-    sim = pf.Simulation(grid, structures=boxes, sources=[src], run_time=2e-15)
+    sim = pf.Simulation(grid, structures=boxes, sources=[src], monitors=list(monitors),
+                        run_time=12e-15, precision=precision)
     if custom:
         sim.eps_r = np.asarray(sim.eps_r) * 1.0
     return sim
@@ -86,6 +88,34 @@ def test_cell1_mode_separate_ade_word():
     want = np.where(ids >= 0, w, 0).astype(np.uint32)
     np.testing.assert_array_equal(t["ade"]["cell_word"], want)
     np.testing.assert_array_equal(t["ade"]["count"], counts)
+
+
+def painted_over_run(precision, custom):
+    """painted_over with a field monitor, a DFT plane and a flux plane."""
+    mons = [pf.FieldMonitor(name="f", components=("Ex", "Ez", "Hy"), interval=7),
+            pf.DFTMonitor(name="d", components=("Ez",), freqs=[C_0 / 1e-6],
+                          plane_axis="x", plane_position=0.12e-6),
+            pf.FluxMonitor(name="fx", plane_axis="x", plane_position=0.12e-6)]
+    return painted_over(custom, precision, mons)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,custom", [("float32", False), ("float64", False),
+                                              ("float32", True)])
+def test_painted_over_medium_runs_bitwise_against_oracle(precision, custom):
+    """The engine takes a dispersive medium with zero cells (its slot kept,
+    nothing allocated) and matches the oracle bit for bit, in table mode and
+    in the per-cell coefficient mode (separate ADE word)."""
+    from oracle import run_oracle
+    sim = painted_over_run(precision, custom)
+    assert np.dtype(sim.dtypes["Ex"]) == np.dtype(precision)
+    res = sim.run()
+    ref = run_oracle(painted_over_run(precision, custom))
+    for c, arr in ref["fields"]["f"].items():
+        assert np.abs(arr).max() > 0
+        np.testing.assert_array_equal(res.fields["f"][c], arr, err_msg=c)
+    np.testing.assert_array_equal(res.dft["d"]["Ez"], ref["dft"]["d"]["Ez"])
+    assert abs(res.flux["fx"] - ref["flux"]["fx"]) <= 1e-6 * max(abs(ref["flux"]["fx"]), 1e-300)
 
 
 def test_rank_helper_errors():
