@@ -480,6 +480,15 @@ int pfs_gemm_bf16(int M, int N, int K, const void *A, int lda, const void *B, in
 int pfs_gemm_bf16_splitk(int M, int N, int K, const void *A, int lda, const void *B, int ldb,
                          float *C, int ldc, float alpha, float beta, int splits, float *work,
                          int64_t work_floats, void *stream);
+/* pfs_gemm_bf16_splitk with either operand stored MN-major: a_mn = 1 means A
+ * is held as its transpose, K x M row-major (lda >= M), b_mn = 1 that B is
+ * held as K x N row-major (ldb >= N). The tensor cores read such an operand
+ * as it lies (no transposed copy): C = alpha * op(A) op(B)^T + beta * C with
+ * the same products in the same order. The backward pass of the surrogate's
+ * layers uses it for dW = dY^T X and dX = dY W. tcgen05 engine only. */
+int pfs_gemm_bf16_ex(int M, int N, int K, const void *A, int lda, int a_mn, const void *B,
+                     int ldb, int b_mn, float *C, int ldc, float alpha, float beta, int splits,
+                     float *work, int64_t work_floats, void *stream);
 /* Selects the tensor-core engine of the two GEMM entry points for the
  * process: 1 = tcgen05.mma with the accumulator in tensor memory (default),
  * 0 = mma.sync m16n8k16 with register accumulators. Other values only query.

@@ -112,6 +112,9 @@ SIGNATURES = {
     "pfs_last_error": (C.c_char_p, []),
     "pfs_gemm_bf16": (C.c_int, [C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp,
                                 C.c_int, C.c_float, C.c_float, _vp]),
+    "pfs_gemm_bf16_ex": (C.c_int, [C.c_int, C.c_int, C.c_int, _vp, C.c_int, C.c_int, _vp,
+                                   C.c_int, C.c_int, _vp, C.c_int, C.c_float, C.c_float,
+                                   C.c_int, _vp, _i64, _vp]),
     "pfs_gemm_bf16_splitk": (C.c_int, [C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int,
                                        _vp, C.c_int, C.c_float, C.c_float, C.c_int, _vp, _i64,
                                        _vp]),

@@ -229,6 +229,18 @@ __device__ __forceinline__ uint64_t tc_desc_sw128(uint32_t saddr) {
          (1ull << 46) | (2ull << 61);
 }
 
+// The same for an MN-major operand (stored K x MN, MN contiguous): TMA puts
+// each 64-element MN strip of a stage (64 K rows of 128 bytes, swizzled in
+// 1024-byte groups of 8 rows) 8192 bytes after the previous one. In the
+// descriptor the leading byte offset is the step between MN strips (8192)
+// and the stride byte offset the step between 8-row K groups (1024); the
+// K = 16 slice ks starts 2048 * ks bytes into the stage.
+constexpr uint32_t kMnStrip = 64 * TBK * 2;  // bytes of one 64-wide MN strip of a stage
+__device__ __forceinline__ uint64_t tc_desc_mn_sw128(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(kMnStrip >> 4) << 16) |
+         ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) | (2ull << 61);
+}
+
 __device__ __forceinline__ void tc_tma_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar,
                                           int x, int y) {
   asm volatile(
@@ -238,12 +250,16 @@ __device__ __forceinline__ void tc_tma_2d(uint32_t dst, const CUtensorMap* map, 
       : "memory");
 }
 
-template <int BN>
+// AMN / BMN: the operand is stored MN-major (K x M or K x N, MN contiguous)
+// and read as such by the tensor cores (the descriptor's transpose bits), so
+// no transposed copy is made; its stage is loaded as 64-wide MN strips.
+template <int BN, bool AMN = false, bool BMN = false>
 __global__ void __launch_bounds__(128, 1)
     k_gemm_tc(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
               int M, int N, int K, float* C, int ldc, float alpha, float beta, int kc, float* work,
               int* err, int wait_test) {
   static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "BN");
+  static_assert(!BMN || BN >= 64, "an MN-major B needs whole 64-wide strips");
   constexpr uint32_t ABYTES = TBM * TBK * 2, SB = tc_stage_bytes(BN);
   extern __shared__ uint8_t tc_smem[];
   __shared__ __align__(8) uint64_t full[TC_STAGES], empty[TC_STAGES], done;
@@ -302,15 +318,28 @@ __global__ void __launch_bounds__(128, 1)
         const uint32_t fb = smem_u32(&full[st]), dst = s0 + st * SB;
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(SB)
                      : "memory");
-        tc_tma_2d(dst, &ta, fb, kbeg + kt * TBK, m0);
-        tc_tma_2d(dst + ABYTES, &tb, fb, kbeg + kt * TBK, n0);
+        if constexpr (AMN) {
+#pragma unroll
+          for (int q = 0; q < TBM / 64; ++q)
+            tc_tma_2d(dst + q * kMnStrip, &ta, fb, m0 + 64 * q, kbeg + kt * TBK);
+        } else {
+          tc_tma_2d(dst, &ta, fb, kbeg + kt * TBK, m0);
+        }
+        if constexpr (BMN) {
+#pragma unroll
+          for (int q = 0; q < BN / 64; ++q)
+            tc_tma_2d(dst + ABYTES + q * kMnStrip, &tb, fb, n0 + 64 * q, kbeg + kt * TBK);
+        } else {
+          tc_tma_2d(dst + ABYTES, &tb, fb, kbeg + kt * TBK, n0);
+        }
       }
       __syncwarp();
     }
     if (lane == 0) n_loaded = kt;
   } else if (warp == 1) {  // MMA issue
-    constexpr uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) |
-                               ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TBM >> 4) << 24);
+    constexpr uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((AMN ? 1u : 0u) << 15) |
+                               ((BMN ? 1u : 0u) << 16) | ((uint32_t)(BN >> 3) << 17) |
+                               ((uint32_t)(TBM >> 4) << 24);
     int kt = 0;
     const bool test_block = wait_test && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0;
     for (; kt < nk; ++kt) {
@@ -327,7 +356,8 @@ __global__ void __launch_bounds__(128, 1)
         const uint32_t a0 = s0 + st * SB, b0 = a0 + ABYTES;
 #pragma unroll
         for (int ks = 0; ks < TBK / 16; ++ks) {
-          const uint64_t da = tc_desc_sw128(a0 + 32 * ks), db = tc_desc_sw128(b0 + 32 * ks);
+          const uint64_t da = AMN ? tc_desc_mn_sw128(a0 + 2048 * ks) : tc_desc_sw128(a0 + 32 * ks);
+          const uint64_t db = BMN ? tc_desc_mn_sw128(b0 + 2048 * ks) : tc_desc_sw128(b0 + 32 * ks);
           const uint32_t accum = (kt > 0 || ks > 0) ? 1u : 0u;
           asm volatile(
               "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
@@ -720,10 +750,45 @@ bool tc_map(CUtensorMap* m, const void* ptr, int cols, int rows, int ld, int box
 int g_gemm_engine = 1;  // 1: tcgen05 (TMEM accumulator), 0: mma.sync m16n8k16
 int g_gemm_wait_test = 0;  // pfs_gemm_wait_test
 
-// Launches the GEMM (split over `sz` K slices of kc when sz > 1).
+template <int BN, bool AMN, bool BMN>
+bool tc_prepare() {
+  return cudaFuncSetAttribute(k_gemm_tc<BN, AMN, BMN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              tc_smem_bytes(BN)) == cudaSuccess;
+}
+
+template <bool AMN, bool BMN>
+void tc_launch(int bn, dim3 grid, cudaStream_t st, const CUtensorMap& ta, const CUtensorMap& tb,
+               int M, int N, int K, float* C, int ldc, float alpha, float beta, int kc,
+               float* work, int* err) {
+  const int wt = g_gemm_wait_test;
+  switch (bn) {
+    case 32:
+      if constexpr (!BMN)
+        k_gemm_tc<32, AMN, BMN><<<grid, 128, tc_smem_bytes(32), st>>>(ta, tb, M, N, K, C, ldc,
+                                                                      alpha, beta, kc, work, err, wt);
+      break;
+    case 64:
+      k_gemm_tc<64, AMN, BMN><<<grid, 128, tc_smem_bytes(64), st>>>(ta, tb, M, N, K, C, ldc, alpha,
+                                                                    beta, kc, work, err, wt);
+      break;
+    case 128:
+      k_gemm_tc<128, AMN, BMN><<<grid, 128, tc_smem_bytes(128), st>>>(ta, tb, M, N, K, C, ldc,
+                                                                      alpha, beta, kc, work, err, wt);
+      break;
+    default:
+      k_gemm_tc<256, AMN, BMN><<<grid, 128, tc_smem_bytes(256), st>>>(ta, tb, M, N, K, C, ldc,
+                                                                      alpha, beta, kc, work, err, wt);
+  }
+}
+
+// Launches the GEMM (split over `sz` K slices of kc when sz > 1). a_mn / b_mn:
+// A is stored K x M (lda >= M), B K x N (ldb >= N), read MN-major by the
+// tensor cores (tcgen05 engine only).
 int launch_gemm(int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B,
                 int ldb, float* C, int ldc, float alpha, float beta, int kc, int sz, float* work,
-                cudaStream_t st) {
+                cudaStream_t st, bool a_mn = false, bool b_mn = false) {
+  if (g_gemm_engine == 0 && (a_mn || b_mn))
+    return sfail(PF_ERR_UNSUPPORTED, "pfs_gemm: MN-major operands need the tcgen05 engine");
   if (g_gemm_engine == 0) {
     const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, sz);
     if (grid.y > 65535) return sfail(PF_ERR_INVALID, "pfs_gemm: M too large");
@@ -735,14 +800,13 @@ int launch_gemm(int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv
     return sfail(PF_ERR_CUDA, "pfs_gemm: cannot resolve the tensor-core error flag");
   static bool attr = false;
   if (!attr) {
-    if (cudaFuncSetAttribute(k_gemm_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             tc_smem_bytes(256)) != cudaSuccess ||
-        cudaFuncSetAttribute(k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             tc_smem_bytes(128)) != cudaSuccess ||
-        cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             tc_smem_bytes(64)) != cudaSuccess ||
-        cudaFuncSetAttribute(k_gemm_tc<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             tc_smem_bytes(32)) != cudaSuccess)
+    if (!(tc_prepare<256, false, false>() && tc_prepare<128, false, false>() &&
+          tc_prepare<64, false, false>() && tc_prepare<32, false, false>() &&
+          tc_prepare<256, true, true>() && tc_prepare<128, true, true>() &&
+          tc_prepare<64, true, true>() && tc_prepare<256, false, true>() &&
+          tc_prepare<128, false, true>() && tc_prepare<64, false, true>() &&
+          tc_prepare<256, true, false>() && tc_prepare<128, true, false>() &&
+          tc_prepare<64, true, false>() && tc_prepare<32, true, false>()))
       return cuda_status("pfs_gemm: shared memory attribute");
     attr = true;
   }
@@ -754,27 +818,22 @@ int launch_gemm(int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv
   // while the grid has fewer blocks than SMs
   int bn = N <= 32 ? 32 : N <= 64 ? 64 : N <= 128 ? 128 : 256;
   while (bn > 32 && gy * ((N + bn - 1) / bn) * sz < 148) bn /= 2;
+  if (b_mn && bn < 64) bn = 64;  // an MN-major B is loaded in 64-wide strips
   CUtensorMap ta, tb;
-  if (!tc_map(&ta, A, K, M, lda, TBM) || !tc_map(&tb, B, K, N, ldb, bn))
-    return sfail(PF_ERR_CUDA, "pfs_gemm: cuTensorMapEncodeTiled failed");
+  // K-major: rows of K elements, box 64 (K) x tile rows; MN-major: rows of
+  // MN elements, box 64 (MN) x 64 (K)
+  const bool ok = (a_mn ? tc_map(&ta, A, M, K, lda, TBK) : tc_map(&ta, A, K, M, lda, TBM)) &&
+                  (b_mn ? tc_map(&tb, B, N, K, ldb, TBK) : tc_map(&tb, B, K, N, ldb, bn));
+  if (!ok) return sfail(PF_ERR_CUDA, "pfs_gemm: cuTensorMapEncodeTiled failed");
   const dim3 grid((N + bn - 1) / bn, (unsigned)gy, sz);
-  switch (bn) {
-    case 32:
-      k_gemm_tc<32><<<grid, 128, tc_smem_bytes(32), st>>>(ta, tb, M, N, K, C, ldc, alpha, beta,
-                                                          kc, work, err, g_gemm_wait_test);
-      break;
-    case 64:
-      k_gemm_tc<64><<<grid, 128, tc_smem_bytes(64), st>>>(ta, tb, M, N, K, C, ldc, alpha, beta,
-                                                          kc, work, err, g_gemm_wait_test);
-      break;
-    case 128:
-      k_gemm_tc<128><<<grid, 128, tc_smem_bytes(128), st>>>(ta, tb, M, N, K, C, ldc, alpha, beta,
-                                                            kc, work, err, g_gemm_wait_test);
-      break;
-    default:
-      k_gemm_tc<256><<<grid, 128, tc_smem_bytes(256), st>>>(ta, tb, M, N, K, C, ldc, alpha, beta,
-                                                            kc, work, err, g_gemm_wait_test);
-  }
+  if (a_mn && b_mn)
+    tc_launch<true, true>(bn, grid, st, ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err);
+  else if (a_mn)
+    tc_launch<true, false>(bn, grid, st, ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err);
+  else if (b_mn)
+    tc_launch<false, true>(bn, grid, st, ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err);
+  else
+    tc_launch<false, false>(bn, grid, st, ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err);
   return PF_OK;
 }
 
@@ -866,6 +925,36 @@ int pfs_gemm_bf16_splitk(int M, int N, int K, const void* A, int lda, const void
   }
   if (rc) return rc;
   return cuda_status("pfs_gemm_bf16_splitk");
+}
+
+int pfs_gemm_bf16_ex(int M, int N, int K, const void* A, int lda, int a_mn, const void* B,
+                     int ldb, int b_mn, float* C, int ldc, float alpha, float beta, int splits,
+                     float* work, int64_t work_floats, void* stream) {
+  if (!a_mn && !b_mn)
+    return pfs_gemm_bf16_splitk(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, splits, work,
+                                work_floats, stream);
+  if (M < 0 || N < 0 || K < 1 || (M && N && (!A || !B || !C)) || splits < 1 || splits > 65535 ||
+      (splits > 1 && !work))
+    return sfail(PF_ERR_INVALID, "pfs_gemm_bf16_ex: bad sizes or NULL operand");
+  if (K % 32 || lda % 8 || ldb % 8 || ldc < N || lda < (a_mn ? M : K) || ldb < (b_mn ? N : K))
+    return sfail(PF_ERR_INVALID,
+                 "pfs_gemm_bf16_ex: K must be a multiple of 32, lda/ldb multiples of 8 and at "
+                 "least the operand's row length");
+  if (!aligned16(A) || !aligned16(B))
+    return sfail(PF_ERR_INVALID, "pfs_gemm_bf16_ex: A and B must be 16-byte aligned");
+  if (splits > 1 && (long long)splits * M * N > work_floats)
+    return sfail(PF_ERR_INVALID, "pfs_gemm_bf16_ex: work holds fewer than splits*M*N floats");
+  if (!M || !N) return PF_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int kc = ((K + splits - 1) / splits + TBK - 1) / TBK * TBK;
+  const int sz = (K + kc - 1) / kc;
+  int rc = launch_gemm(M, N, K, (const __nv_bfloat16*)A, lda, (const __nv_bfloat16*)B, ldb, C,
+                       ldc, alpha, beta, sz == 1 ? K : kc, sz, sz == 1 ? nullptr : work, st,
+                       a_mn != 0, b_mn != 0);
+  if (!rc && sz > 1)
+    k_splitk_reduce<<<grid_for((long long)M * N, 256), 256, 0, st>>>(M, N, sz, work, C, ldc, beta);
+  if (rc) return rc;
+  return cuda_status("pfs_gemm_bf16_ex");
 }
 
 int pfs_im2col(int nb, int H, int W, int C, int kh, int kw, int stride, int ph, int pw,

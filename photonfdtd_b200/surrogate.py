@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 import time
 from dataclasses import dataclass
 from typing import Callable, Dict, List, Optional, Sequence, Tuple
@@ -147,6 +148,9 @@ class SurrogateNet:
         self.dev = device
         self.layers = plan()
         self.L = N.lib()
+        # backward GEMMs read dY, the lowered input and W MN-major (no
+        # transposed copies); PFB200_SURROGATE_TRANSPOSE=1 restores the copies
+        self.mn_major = not os.environ.get("PFB200_SURROGATE_TRANSPOSE")
         if params is None:
             params = init_params(self.layers, seed)
         self._alloc(params)
@@ -196,9 +200,11 @@ class SurrogateNet:
             self.y32.append(t.zeros((M, cp), dtype=f32, device=dev))
             self.y16.append(t.zeros((M, cp), dtype=bf, device=dev))
             self.d16.append(t.zeros((M, cp), dtype=bf, device=dev))
-            self.dT.append(t.zeros((cp, M), dtype=bf, device=dev))
-            self.colT.append(t.zeros((Kp, M), dtype=bf, device=dev))
-            self.wT.append(t.zeros((Kp, cp), dtype=bf, device=dev))
+            # transposed copies only for the path that makes them
+            tr = not self.mn_major
+            self.dT.append(t.zeros((cp, M), dtype=bf, device=dev) if tr else None)
+            self.colT.append(t.zeros((Kp, M), dtype=bf, device=dev) if tr else None)
+            self.wT.append(t.zeros((Kp, cp), dtype=bf, device=dev) if tr else None)
             self.dcol.append(t.zeros((M, Kp), dtype=f32, device=dev))
             self.dx.append(t.zeros((B * L.H * L.W * L.cin,), dtype=f32, device=dev))
             rb = int(min(65535, max(1, M // 64)))
@@ -294,22 +300,23 @@ class SurrogateNet:
                                      self._p(part), rb, s))
             # weight gradient: dW = d^T col (K of the GEMM = M rows)
             A = self.col[li] if L.kind == "conv" else self.y16[li - 1]
-            self._chk(L_.pfs_transpose_bf16(M, L.coutp, self._p(self.d16[li]), L.coutp,
-                                            self._p(self.dT[li]), M, s))
-            self._chk(L_.pfs_transpose_bf16(M, L.Kp, self._p(A), L.Kp, self._p(self.colT[li]), M,
-                                            s))
-            self._chk(L_.pfs_gemm_bf16_splitk(L.coutp, L.Kp, M, self._p(self.dT[li]), M,
-                                              self._p(self.colT[li]), M, self._p(self.gw[li]),
+            if self.mn_major:
+                # the tensor cores read d and col as they lie (MN-major)
+                self._chk(L_.pfs_gemm_bf16_ex(L.coutp, L.Kp, M, self._p(self.d16[li]), L.coutp,
+                                              1, self._p(A), L.Kp, 1, self._p(self.gw[li]),
                                               L.Kp, 1.0, 0.0, self.splits[li],
                                               self._p(self.work), self.work.numel(), s))
-            if first and not input_grad:
-                break
-            # input gradient: dcol = d W, then col2im
-            self._chk(L_.pfs_transpose_bf16(L.coutp, L.Kp, self._p(self.w16[li]), L.Kp,
-                                            self._p(self.wT[li]), L.coutp, s))
-            self._chk(L_.pfs_gemm_bf16(M, L.Kp, L.coutp, self._p(self.d16[li]), L.coutp,
-                                       self._p(self.wT[li]), L.coutp, self._p(self.dcol[li]),
-                                       L.Kp, 1.0, 0.0, s))
+                if first and not input_grad:
+                    break
+                # input gradient: dcol = d W, W read MN-major
+                self._chk(L_.pfs_gemm_bf16_ex(M, L.Kp, L.coutp, self._p(self.d16[li]), L.coutp,
+                                              0, self._p(self.w16[li]), L.Kp, 1,
+                                              self._p(self.dcol[li]), L.Kp, 1.0, 0.0, 1, None,
+                                              0, s))
+            else:
+                self._transposed_grads(li, L, M, A, s, not first or input_grad)
+                if first and not input_grad:
+                    break
             if L.kind == "conv":
                 self._chk(L_.pfs_col2im(self.B, L.H, L.W, L.cin, L.kh, L.kw, L.stride, L.ph, L.pw,
                                         self._p(self.dcol[li]), L.Kp, self._p(self.dx[li]), s))
@@ -319,6 +326,26 @@ class SurrogateNet:
         if input_grad:
             return self.dx[0].view(self.B, 64, 64)
         return None
+
+    def _transposed_grads(self, li, L, M, A, s, need_dcol: bool) -> None:
+        """dW (and dcol when need_dcol) through explicit BF16 transposes and
+        K-major GEMMs: the form before MN-major operands, kept for comparison
+        (PFB200_SURROGATE_TRANSPOSE=1)."""
+        L_ = self.L
+        self._chk(L_.pfs_transpose_bf16(M, L.coutp, self._p(self.d16[li]), L.coutp,
+                                        self._p(self.dT[li]), M, s))
+        self._chk(L_.pfs_transpose_bf16(M, L.Kp, self._p(A), L.Kp, self._p(self.colT[li]), M, s))
+        self._chk(L_.pfs_gemm_bf16_splitk(L.coutp, L.Kp, M, self._p(self.dT[li]), M,
+                                          self._p(self.colT[li]), M, self._p(self.gw[li]),
+                                          L.Kp, 1.0, 0.0, self.splits[li],
+                                          self._p(self.work), self.work.numel(), s))
+        if not need_dcol:
+            return
+        self._chk(L_.pfs_transpose_bf16(L.coutp, L.Kp, self._p(self.w16[li]), L.Kp,
+                                        self._p(self.wT[li]), L.coutp, s))
+        self._chk(L_.pfs_gemm_bf16(M, L.Kp, L.coutp, self._p(self.d16[li]), L.coutp,
+                                   self._p(self.wT[li]), L.coutp, self._p(self.dcol[li]),
+                                   L.Kp, 1.0, 0.0, s))
 
     def adam_step(self, lr: float, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8,
                   wd: float = 0.0) -> None:

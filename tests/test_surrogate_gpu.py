@@ -1,5 +1,5 @@
 """Surrogate kernels on the GPU against NumPy: the BF16 tensor-core GEMM at
-FP32-accumulation accuracy, the convolution lowering and its adjoint, the
+FP32-accumulation accuracy (K-major and MN-major operands), the convolution lowering and its adjoint, the
 elementwise / reduction kernels, Adam, and the whole network's forward and
 reverse pass against the NumPy oracle (oracle/surrogate_ref.py) run with the
 same BF16 rounding of GEMM operands. A short training run must cut the loss."""
@@ -89,6 +89,77 @@ def test_gemm_bf16_splitk(M, Nn, K, splits, beta, engine):
     assert np.max(np.abs(outs[0] - want)) <= 1e-5 * np.max(np.abs(want)) * np.sqrt(K)
     assert N.lib().pfs_gemm_bf16_splitk(M, Nn, K, _p(dA), K, _p(dB), K, _p(dC), Nn, 1.0, beta,
                                         splits, _p(work), 10, _s()) == N.PF_ERR_INVALID
+
+
+@pytest.mark.parametrize("a_mn,b_mn", [(1, 1), (1, 0), (0, 1)])
+@pytest.mark.parametrize("M,Nn,K,splits", [(128, 64, 4096, 1), (96, 1152, 8192, 6),
+                                           (1000, 200, 160, 1), (296, 96, 544, 3),
+                                           (256, 256, 2048, 1)])
+def test_gemm_mn_major_operands(M, Nn, K, splits, a_mn, b_mn):
+    """pfs_gemm_bf16_ex with A held as K x M and / or B as K x N (read
+    MN-major by the tensor cores) against NumPy, and bit for bit against the
+    K-major GEMM on transposed copies (same products, same order)."""
+    t = _t()
+    L = N.lib()
+    rng = np.random.default_rng(M * 7 + Nn + K + 3 * a_mn + b_mn)
+    A = bf16(rng.standard_normal((M, K)))
+    B = bf16(rng.standard_normal((Nn, K)))
+    C0 = rng.standard_normal((M, Nn)).astype(np.float32)
+    dev = lambda a: t.from_numpy(np.ascontiguousarray(a).astype(np.float32)).cuda().to(t.bfloat16)  # noqa: E731
+    dA, dB, dAt, dBt = dev(A), dev(B), dev(A.T), dev(B.T)
+    work = t.empty(max(1, splits) * M * Nn, dtype=t.float32, device="cuda")
+    cnt = C.c_int(0)
+    _chk(L.pfs_gemm_timeouts(C.byref(cnt), 1))
+    dC = t.from_numpy(C0.copy()).cuda()
+    _chk(L.pfs_gemm_bf16_ex(M, Nn, K, _p(dAt if a_mn else dA), M if a_mn else K, a_mn,
+                            _p(dBt if b_mn else dB), Nn if b_mn else K, b_mn, _p(dC), Nn, 1.0,
+                            0.5, splits, _p(work), work.numel(), _s()))
+    got = dC.cpu().numpy()
+    dK = t.from_numpy(C0.copy()).cuda()
+    _chk(L.pfs_gemm_bf16_splitk(M, Nn, K, _p(dA), K, _p(dB), K, _p(dK), Nn, 1.0, 0.5, splits,
+                                _p(work), work.numel(), _s()))
+    _chk(L.pfs_gemm_timeouts(C.byref(cnt), 1))
+    assert cnt.value == 0
+    want = A @ B.T + 0.5 * C0
+    assert np.max(np.abs(got - want)) <= 1e-5 * np.max(np.abs(want)) * np.sqrt(K)
+    np.testing.assert_array_equal(got, dK.cpu().numpy())
+
+
+def test_gemm_mn_major_rejects_short_rows():
+    t = _t()
+    L = N.lib()
+    a = t.zeros((64, 128), dtype=t.bfloat16, device="cuda")
+    c = t.zeros((128, 64), dtype=t.float32, device="cuda")
+    # A held as K x M needs lda >= M
+    assert L.pfs_gemm_bf16_ex(128, 64, 64, _p(a), 64, 1, _p(a), 128, 1, _p(c), 64, 1.0, 0.0, 1,
+                              None, 0, _s()) == N.PF_ERR_INVALID
+
+
+def test_backward_mn_major_equals_transposed_copies(monkeypatch):
+    """The network's reverse pass with MN-major GEMM operands gives the same
+    weight and input gradients, bit for bit, as with explicit transposes."""
+    t = _t()
+    layers = plan()
+    params = [(None if w is None else bf16(w), b) for w, b in init_params(layers, seed=8)]
+    rng = np.random.default_rng(9)
+    x = t.from_numpy(bf16(rng.uniform(-1, 1, (32, 64, 64))).astype(np.float32)).cuda()
+    R = t.from_numpy(rng.standard_normal((32, 32, 2)).astype(np.float32)).cuda()
+    out = []
+    for tr in (False, True):
+        if tr:
+            monkeypatch.setenv("PFB200_SURROGATE_TRANSPOSE", "1")
+        net = SurrogateNet(32, params=params)
+        assert net.mn_major == (not tr)
+        net.forward(x)
+        net.set_output_grad(R)
+        dx = net.backward(input_grad=True).cpu().numpy()
+        out.append((dx, [(None if g is None else g.copy(), b.copy() if b is not None else None)
+                         for g, b in net.grads()]))
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    for (g0, b0), (g1, b1) in zip(out[0][1], out[1][1]):
+        if g0 is not None:
+            np.testing.assert_array_equal(g0, g1)
+            np.testing.assert_array_equal(b0, b1)
 
 
 def test_gemm_rejects_bad_shapes():
