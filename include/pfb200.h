@@ -489,6 +489,14 @@ int pfs_gemm_bf16_splitk(int M, int N, int K, const void *A, int lda, const void
 int pfs_gemm_bf16_ex(int M, int N, int K, const void *A, int lda, int a_mn, const void *B,
                      int ldb, int b_mn, float *C, int ldc, float alpha, float beta, int splits,
                      float *work, int64_t work_floats, void *stream);
+/* A layer's forward GEMM with pfs_bias_act fused into its epilogue:
+ * y32 = act(A B^T + bias) (FP32, ld ldy) and, when y16 is not NULL, the
+ * same values in BF16 (ld ldy); bias may be NULL, relu != 0 applies ReLU.
+ * Equal bit for bit to pfs_gemm_bf16 (alpha 1, beta 0) then pfs_bias_act.
+ * tcgen05 engine only. */
+int pfs_gemm_bf16_bias_act(int M, int N, int K, const void *A, int lda, const void *B, int ldb,
+                           const float *bias, int relu, float *y32, void *y16, int ldy,
+                           void *stream);
 /* Selects the tensor-core engine of the two GEMM entry points for the
  * process: 1 = tcgen05.mma with the accumulator in tensor memory (default),
  * 0 = mma.sync m16n8k16 with register accumulators. Other values only query.

@@ -115,6 +115,8 @@ SIGNATURES = {
     "pfs_gemm_bf16_ex": (C.c_int, [C.c_int, C.c_int, C.c_int, _vp, C.c_int, C.c_int, _vp,
                                    C.c_int, C.c_int, _vp, C.c_int, C.c_float, C.c_float,
                                    C.c_int, _vp, _i64, _vp]),
+    "pfs_gemm_bf16_bias_act": (C.c_int, [C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int,
+                                         _vp, C.c_int, _vp, _vp, C.c_int, _vp]),
     "pfs_gemm_bf16_splitk": (C.c_int, [C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp, C.c_int,
                                        _vp, C.c_int, C.c_float, C.c_float, C.c_int, _vp, _i64,
                                        _vp]),

@@ -250,14 +250,23 @@ __device__ __forceinline__ void tc_tma_2d(uint32_t dst, const CUtensorMap* map, 
       : "memory");
 }
 
+// Epilogue of a layer's forward GEMM (EPI): y = act(C + bias) written as
+// FP32 (to C) and BF16 (y16, same leading dimension), k_bias_act's
+// arithmetic on the value C would have held; beta is 0 and K unsplit.
+struct TcEpi {
+  const float* bias;
+  int relu;
+  __nv_bfloat16* y16;
+};
+
 // AMN / BMN: the operand is stored MN-major (K x M or K x N, MN contiguous)
 // and read as such by the tensor cores (the descriptor's transpose bits), so
 // no transposed copy is made; its stage is loaded as 64-wide MN strips.
-template <int BN, bool AMN = false, bool BMN = false>
+template <int BN, bool AMN = false, bool BMN = false, bool EPI = false>
 __global__ void __launch_bounds__(128, 1)
     k_gemm_tc(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
               int M, int N, int K, float* C, int ldc, float alpha, float beta, int kc, float* work,
-              int* err, int wait_test) {
+              int* err, int wait_test, TcEpi ep) {
   static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "BN");
   static_assert(!BMN || BN >= 64, "an MN-major B needs whole 64-wide strips");
   constexpr uint32_t ABYTES = TBM * TBK * 2, SB = tc_stage_bytes(BN);
@@ -419,7 +428,14 @@ __global__ void __launch_bounds__(128, 1)
         if (r < M && n < N) {
           float* o = C + (long long)r * ldc + n;
           const float val = alpha * stage[rr * 33 + lane];
-          *o = beta == 0.f ? val : val + beta * *o;
+          if constexpr (EPI) {
+            float v = val + (ep.bias ? ep.bias[n] : 0.f);
+            if (ep.relu) v = fmaxf(v, 0.f);
+            *o = v;
+            if (ep.y16) ep.y16[(long long)r * ldc + n] = __float2bfloat16(v);
+          } else {
+            *o = beta == 0.f ? val : val + beta * *o;
+          }
         }
       }
       __syncwarp();
@@ -750,34 +766,35 @@ bool tc_map(CUtensorMap* m, const void* ptr, int cols, int rows, int ld, int box
 int g_gemm_engine = 1;  // 1: tcgen05 (TMEM accumulator), 0: mma.sync m16n8k16
 int g_gemm_wait_test = 0;  // pfs_gemm_wait_test
 
-template <int BN, bool AMN, bool BMN>
+template <int BN, bool AMN, bool BMN, bool EPI = false>
 bool tc_prepare() {
-  return cudaFuncSetAttribute(k_gemm_tc<BN, AMN, BMN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  return cudaFuncSetAttribute(k_gemm_tc<BN, AMN, BMN, EPI>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                               tc_smem_bytes(BN)) == cudaSuccess;
 }
 
-template <bool AMN, bool BMN>
+template <bool AMN, bool BMN, bool EPI = false>
 void tc_launch(int bn, dim3 grid, cudaStream_t st, const CUtensorMap& ta, const CUtensorMap& tb,
                int M, int N, int K, float* C, int ldc, float alpha, float beta, int kc,
-               float* work, int* err) {
+               float* work, int* err, TcEpi ep = TcEpi{}) {
   const int wt = g_gemm_wait_test;
   switch (bn) {
     case 32:
       if constexpr (!BMN)
-        k_gemm_tc<32, AMN, BMN><<<grid, 128, tc_smem_bytes(32), st>>>(ta, tb, M, N, K, C, ldc,
-                                                                      alpha, beta, kc, work, err, wt);
+        k_gemm_tc<32, AMN, BMN, EPI><<<grid, 128, tc_smem_bytes(32), st>>>(
+            ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err, wt, ep);
       break;
     case 64:
-      k_gemm_tc<64, AMN, BMN><<<grid, 128, tc_smem_bytes(64), st>>>(ta, tb, M, N, K, C, ldc, alpha,
-                                                                    beta, kc, work, err, wt);
+      k_gemm_tc<64, AMN, BMN, EPI><<<grid, 128, tc_smem_bytes(64), st>>>(
+          ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err, wt, ep);
       break;
     case 128:
-      k_gemm_tc<128, AMN, BMN><<<grid, 128, tc_smem_bytes(128), st>>>(ta, tb, M, N, K, C, ldc,
-                                                                      alpha, beta, kc, work, err, wt);
+      k_gemm_tc<128, AMN, BMN, EPI><<<grid, 128, tc_smem_bytes(128), st>>>(
+          ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err, wt, ep);
       break;
     default:
-      k_gemm_tc<256, AMN, BMN><<<grid, 128, tc_smem_bytes(256), st>>>(ta, tb, M, N, K, C, ldc,
-                                                                      alpha, beta, kc, work, err, wt);
+      k_gemm_tc<256, AMN, BMN, EPI><<<grid, 128, tc_smem_bytes(256), st>>>(
+          ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err, wt, ep);
   }
 }
 
@@ -786,7 +803,11 @@ void tc_launch(int bn, dim3 grid, cudaStream_t st, const CUtensorMap& ta, const 
 // tensor cores (tcgen05 engine only).
 int launch_gemm(int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B,
                 int ldb, float* C, int ldc, float alpha, float beta, int kc, int sz, float* work,
-                cudaStream_t st, bool a_mn = false, bool b_mn = false) {
+                cudaStream_t st, bool a_mn = false, bool b_mn = false,
+                const TcEpi* epi = nullptr) {
+  if (epi && (g_gemm_engine == 0 || a_mn || b_mn || sz != 1 || beta != 0.f))
+    return sfail(PF_ERR_UNSUPPORTED, "pfs_gemm: the fused epilogue needs the tcgen05 engine, "
+                                     "K-major operands, one K slice and beta = 0");
   if (g_gemm_engine == 0 && (a_mn || b_mn))
     return sfail(PF_ERR_UNSUPPORTED, "pfs_gemm: MN-major operands need the tcgen05 engine");
   if (g_gemm_engine == 0) {
@@ -806,7 +827,9 @@ int launch_gemm(int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv
           tc_prepare<64, true, true>() && tc_prepare<256, false, true>() &&
           tc_prepare<128, false, true>() && tc_prepare<64, false, true>() &&
           tc_prepare<256, true, false>() && tc_prepare<128, true, false>() &&
-          tc_prepare<64, true, false>() && tc_prepare<32, true, false>()))
+          tc_prepare<64, true, false>() && tc_prepare<32, true, false>() &&
+          tc_prepare<256, false, false, true>() && tc_prepare<128, false, false, true>() &&
+          tc_prepare<64, false, false, true>() && tc_prepare<32, false, false, true>()))
       return cuda_status("pfs_gemm: shared memory attribute");
     attr = true;
   }
@@ -826,7 +849,10 @@ int launch_gemm(int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv
                   (b_mn ? tc_map(&tb, B, N, K, ldb, TBK) : tc_map(&tb, B, K, N, ldb, bn));
   if (!ok) return sfail(PF_ERR_CUDA, "pfs_gemm: cuTensorMapEncodeTiled failed");
   const dim3 grid((N + bn - 1) / bn, (unsigned)gy, sz);
-  if (a_mn && b_mn)
+  if (epi)
+    tc_launch<false, false, true>(bn, grid, st, ta, tb, M, N, K, C, ldc, alpha, beta, kc, work,
+                                  err, *epi);
+  else if (a_mn && b_mn)
     tc_launch<true, true>(bn, grid, st, ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err);
   else if (a_mn)
     tc_launch<true, false>(bn, grid, st, ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err);
@@ -955,6 +981,26 @@ int pfs_gemm_bf16_ex(int M, int N, int K, const void* A, int lda, int a_mn, cons
     k_splitk_reduce<<<grid_for((long long)M * N, 256), 256, 0, st>>>(M, N, sz, work, C, ldc, beta);
   if (rc) return rc;
   return cuda_status("pfs_gemm_bf16_ex");
+}
+
+int pfs_gemm_bf16_bias_act(int M, int N, int K, const void* A, int lda, const void* B, int ldb,
+                           const float* bias, int relu, float* y32, void* y16, int ldy,
+                           void* stream) {
+  if (M < 0 || N < 0 || K < 1 || (M && N && (!A || !B || !y32)))
+    return sfail(PF_ERR_INVALID, "pfs_gemm_bf16_bias_act: bad sizes or NULL operand");
+  if (K % 32 || lda % 8 || ldb % 8 || lda < K || ldb < K || ldy < N)
+    return sfail(PF_ERR_INVALID,
+                 "pfs_gemm_bf16_bias_act: K must be a multiple of 32, lda/ldb multiples of 8 "
+                 "and >= K");
+  if (!aligned16(A) || !aligned16(B))
+    return sfail(PF_ERR_INVALID, "pfs_gemm_bf16_bias_act: A and B must be 16-byte aligned");
+  if (!M || !N) return PF_OK;
+  const TcEpi ep{bias, relu, (__nv_bfloat16*)y16};
+  const int rc = launch_gemm(M, N, K, (const __nv_bfloat16*)A, lda, (const __nv_bfloat16*)B,
+                             ldb, y32, ldy, 1.0f, 0.0f, K, 1, nullptr, (cudaStream_t)stream,
+                             false, false, &ep);
+  if (rc) return rc;
+  return cuda_status("pfs_gemm_bf16_bias_act");
 }
 
 int pfs_im2col(int nb, int H, int W, int C, int kh, int kw, int stride, int ph, int pw,

@@ -151,6 +151,9 @@ class SurrogateNet:
         # backward GEMMs read dY, the lowered input and W MN-major (no
         # transposed copies); PFB200_SURROGATE_TRANSPOSE=1 restores the copies
         self.mn_major = not os.environ.get("PFB200_SURROGATE_TRANSPOSE")
+        # PFB200_SURROGATE_FUSED=1: bias + activation in the forward GEMM's
+        # epilogue (pfs_gemm_bf16_bias_act) instead of a separate pass
+        self.fused_epilogue = bool(os.environ.get("PFB200_SURROGATE_FUSED"))
         if params is None:
             params = init_params(self.layers, seed)
         self._alloc(params)
@@ -257,10 +260,19 @@ class SurrogateNet:
                 A = self.col[li]
             else:
                 A = inp
-            self._chk(L_.pfs_gemm_bf16(M, L.coutp, L.Kp, self._p(A), L.Kp, self._p(self.w16[li]),
-                                       L.Kp, self._p(self.cpre[li]), L.coutp, 1.0, 0.0, s))
-            self._chk(L_.pfs_bias_act(M, L.coutp, self._p(self.cpre[li]), self._p(self.b32[li]),
-                                      int(L.relu), self._p(self.y32[li]), self._p(self.y16[li]), s))
+            if self.fused_epilogue:
+                self._chk(L_.pfs_gemm_bf16_bias_act(M, L.coutp, L.Kp, self._p(A), L.Kp,
+                                                    self._p(self.w16[li]), L.Kp,
+                                                    self._p(self.b32[li]), int(L.relu),
+                                                    self._p(self.y32[li]), self._p(self.y16[li]),
+                                                    L.coutp, s))
+            else:
+                self._chk(L_.pfs_gemm_bf16(M, L.coutp, L.Kp, self._p(A), L.Kp,
+                                           self._p(self.w16[li]), L.Kp, self._p(self.cpre[li]),
+                                           L.coutp, 1.0, 0.0, s))
+                self._chk(L_.pfs_bias_act(M, L.coutp, self._p(self.cpre[li]),
+                                          self._p(self.b32[li]), int(L.relu),
+                                          self._p(self.y32[li]), self._p(self.y16[li]), s))
             inp = self.y16[li]
         self._last = li
         return self.y32[-1].view(self.B, N_FREQ, 32)[:, :, :2]

@@ -162,6 +162,48 @@ def test_backward_mn_major_equals_transposed_copies(monkeypatch):
             np.testing.assert_array_equal(b0, b1)
 
 
+@pytest.mark.parametrize("M,Nn,K,relu", [(1000, 200, 160, 1), (8192, 256, 1152, 1),
+                                          (96, 64, 2048, 0), (4096, 32, 32, 1)])
+def test_gemm_bias_act_epilogue(M, Nn, K, relu):
+    """The forward GEMM with bias + activation in its epilogue equals the
+    GEMM followed by pfs_bias_act, bit for bit, in FP32 and BF16."""
+    t = _t()
+    L = N.lib()
+    rng = np.random.default_rng(M + Nn + K + relu)
+    dA = t.from_numpy(bf16(rng.standard_normal((M, K))).astype(np.float32)).cuda().to(t.bfloat16)
+    dB = t.from_numpy(bf16(rng.standard_normal((Nn, K))).astype(np.float32)).cuda().to(t.bfloat16)
+    bias = t.from_numpy(rng.standard_normal(Nn).astype(np.float32)).cuda()
+    y32, y16 = t.empty((M, Nn), device="cuda"), t.empty((M, Nn), dtype=t.bfloat16, device="cuda")
+    _chk(L.pfs_gemm_bf16_bias_act(M, Nn, K, _p(dA), K, _p(dB), K, _p(bias), relu, _p(y32),
+                                  _p(y16), Nn, _s()))
+    pre = t.empty((M, Nn), device="cuda")
+    r32, r16 = t.empty_like(y32), t.empty_like(y16)
+    _chk(L.pfs_gemm_bf16(M, Nn, K, _p(dA), K, _p(dB), K, _p(pre), Nn, 1.0, 0.0, _s()))
+    _chk(L.pfs_bias_act(M, Nn, _p(pre), _p(bias), relu, _p(r32), _p(r16), _s()))
+    assert t.equal(y32, r32) and t.equal(y16.view(t.int16), r16.view(t.int16))
+
+
+def test_forward_fused_epilogue_equals_separate_pass(monkeypatch):
+    """The network's forward with the fused epilogue equals the separate
+    bias + activation pass bit for bit (every layer's FP32 output)."""
+    t = _t()
+    layers = plan()
+    params = [(None if w is None else bf16(w), b) for w, b in init_params(layers, seed=10)]
+    x = t.from_numpy(bf16(np.random.default_rng(11).uniform(-1, 1, (32, 64, 64)))
+                     .astype(np.float32)).cuda()
+    outs = []
+    for fused in (False, True):
+        if fused:
+            monkeypatch.setenv("PFB200_SURROGATE_FUSED", "1")
+        net = SurrogateNet(32, params=params)
+        assert net.fused_epilogue == fused
+        net.forward(x)
+        outs.append([None if y is None else y.cpu().numpy() for y in net.y32])
+    for a, b in zip(*outs):
+        if a is not None:
+            np.testing.assert_array_equal(a, b)
+
+
 def test_gemm_rejects_bad_shapes():
     L = N.lib()
     assert L.pfs_gemm_bf16(4, 4, 20, 16, 20, 16, 20, 16, 4, 1.0, 0.0, None) == N.PF_ERR_INVALID
