@@ -489,7 +489,8 @@ int pfs_gemm_bf16_splitk(int M, int N, int K, const void *A, int lda, const void
 int pfs_gemm_bf16_ex(int M, int N, int K, const void *A, int lda, int a_mn, const void *B,
                      int ldb, int b_mn, float *C, int ldc, float alpha, float beta, int splits,
                      float *work, int64_t work_floats, void *stream);
-/* A layer's forward GEMM with pfs_bias_act fused into its epilogue:
+/* A layer's forward GEMM with pfs_bias_act fused into its epilogue (the
+ * surrogate network's forward pass uses it):
  * y32 = act(A B^T + bias) (FP32, ld ldy) and, when y16 is not NULL, the
  * same values in BF16 (ld ldy); bias may be NULL, relu != 0 applies ReLU.
  * Equal bit for bit to pfs_gemm_bf16 (alpha 1, beta 0) then pfs_bias_act.

@@ -151,9 +151,10 @@ class SurrogateNet:
         # backward GEMMs read dY, the lowered input and W MN-major (no
         # transposed copies); PFB200_SURROGATE_TRANSPOSE=1 restores the copies
         self.mn_major = not os.environ.get("PFB200_SURROGATE_TRANSPOSE")
-        # PFB200_SURROGATE_FUSED=1: bias + activation in the forward GEMM's
-        # epilogue (pfs_gemm_bf16_bias_act) instead of a separate pass
-        self.fused_epilogue = bool(os.environ.get("PFB200_SURROGATE_FUSED"))
+        # bias + activation in the forward GEMM's epilogue
+        # (pfs_gemm_bf16_bias_act); PFB200_SURROGATE_UNFUSED=1 runs the
+        # separate pass instead
+        self.fused_epilogue = not os.environ.get("PFB200_SURROGATE_UNFUSED")
         if params is None:
             params = init_params(self.layers, seed)
         self._alloc(params)

@@ -194,7 +194,9 @@ def test_forward_fused_epilogue_equals_separate_pass(monkeypatch):
     outs = []
     for fused in (False, True):
         if fused:
-            monkeypatch.setenv("PFB200_SURROGATE_FUSED", "1")
+            monkeypatch.delenv("PFB200_SURROGATE_UNFUSED", raising=False)
+        else:
+            monkeypatch.setenv("PFB200_SURROGATE_UNFUSED", "1")
         net = SurrogateNet(32, params=params)
         assert net.fused_epilogue == fused
         net.forward(x)
