@@ -18,7 +18,12 @@ NAMES = ["tm2d_f32", "cube3d_f64", "xz2d_f32", "line1d_f64", "disp2d_f32", "sub3
          "cube3d_f32", "tm2d_f64"]
 
 
-def test_concurrent_runs_equal_single_runs():
+@pytest.mark.parametrize("pipelined", [False, True])
+def test_concurrent_runs_equal_single_runs(pipelined, monkeypatch):
+    """Both with the scenes' preparation in the workers (the default) and
+    prepared one after another first (PFB200_RUN_MANY_SERIAL_PREP)."""
+    if not pipelined:
+        monkeypatch.setenv("PFB200_RUN_MANY_SERIAL_PREP", "1")
     together = run_many([scenes.build(n, pf) for n in NAMES], workers=4)
     for name, res in zip(NAMES, together):
         alone = run_b200(scenes.build(name, pf))
