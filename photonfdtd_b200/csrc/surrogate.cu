@@ -167,8 +167,9 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(int M, int N, int K, const __
 // columns x 128 lanes) from tcgen05.mma.cta_group::1.kind::f16 (BF16 in, FP32
 // accumulate). Operand tiles of 64 K-columns (128-byte rows) arrive by TMA
 // (cp.async.bulk.tensor, 128-byte swizzle, zeros past the matrix edge) in a
-// ring of TC_STAGES stages: warp 0 produces (waits for a stage's `empty`
-// barrier, posts the byte count on its `full` barrier, issues the two loads),
+// ring of up to TC_STAGES stages (tc_ring_stages): warp 0 produces (waits
+// for a stage's `empty` barrier, posts the byte count on its `full`
+// barrier, issues the two loads),
 // warp 1 consumes (waits for `full`, lane 0 issues four K = 16 MMAs and
 // commits them to `empty`, so the stage is refilled once they have read it).
 // A last commit to `done` releases all four warps into the epilogue: each
@@ -186,8 +187,17 @@ constexpr int TBM = 128, TBK = 64, TC_STAGES = 4;
 constexpr unsigned long long kTcWaitNs = 1000000000ull;  // 1 s per wait
 
 __host__ __device__ constexpr int tc_stage_bytes(int bn) { return (TBM + bn) * TBK * 2; }
-__host__ __device__ constexpr int tc_smem_bytes(int bn) {
-  return TC_STAGES * tc_stage_bytes(bn) + 1024;  // + alignment of the ring to 1024 bytes
+__host__ __device__ constexpr int tc_smem_bytes(int bn, int stages = TC_STAGES) {
+  return stages * tc_stage_bytes(bn) + 1024;  // + alignment of the ring to 1024 bytes
+}
+// Ring depth of a launch: no more stages than K tiles in a block's slice, so
+// a short-K GEMM (a layer's input gradient: K = 32..256) takes less shared
+// memory and several blocks share an SM (one block's epilogue overlapping
+// another's loads and MMAs) instead of one block per SM leaving it idle.
+// PFB200_TC_FULL_RING=1 keeps the full ring for every launch (comparison).
+inline int tc_ring_stages(int kc) {
+  static const bool full = getenv("PFB200_TC_FULL_RING") != nullptr;
+  return full ? TC_STAGES : std::max(1, std::min(TC_STAGES, (kc + TBK - 1) / TBK));
 }
 
 __device__ __forceinline__ unsigned long long tc_now() {
@@ -266,7 +276,7 @@ template <int BN, bool AMN = false, bool BMN = false, bool EPI = false>
 __global__ void __launch_bounds__(128, 1)
     k_gemm_tc(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
               int M, int N, int K, float* C, int ldc, float alpha, float beta, int kc, float* work,
-              int* err, int wait_test, TcEpi ep) {
+              int* err, int wait_test, TcEpi ep, int nst) {
   static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "BN");
   static_assert(!BMN || BN >= 64, "an MN-major B needs whole 64-wide strips");
   constexpr uint32_t ABYTES = TBM * TBK * 2, SB = tc_stage_bytes(BN);
@@ -283,10 +293,10 @@ __global__ void __launch_bounds__(128, 1)
   const int m0 = blockIdx.y * TBM, n0 = blockIdx.x * BN;
   const int kbeg = blockIdx.z * kc;
   const int kend = min(K, kbeg + kc);
-  if (gridDim.z > 1) {
+  if (gridDim.z > 1) {  // split K (never with the fused epilogue)
     C = work + (long long)blockIdx.z * M * N;
     ldc = N;
-    beta = 0.f;
+    if constexpr (!EPI) beta = 0.f;
   }
   const int nk = (kend - kbeg + TBK - 1) / TBK;  // >= 1 (host guarantees non-empty slices)
   const uint32_t s0 = (smem_u32(tc_smem) + 1023u) & ~1023u;
@@ -315,10 +325,9 @@ __global__ void __launch_bounds__(128, 1)
   if (warp == 0) {  // producer
     int kt = 0;
     for (; kt < nk; ++kt) {
-      const int st = kt % TC_STAGES;
+      const int st = kt % nst;
       bool ok = true;
-      if (kt >= TC_STAGES)
-        ok = tc_mbar_wait(smem_u32(&empty[st]), ((kt / TC_STAGES) - 1) & 1, abort_v);
+      if (kt >= nst) ok = tc_mbar_wait(smem_u32(&empty[st]), ((kt / nst) - 1) & 1, abort_v);
       if (!__all_sync(0xffffffffu, ok && !*abort_v)) {
         if (lane == 0) *abort_v = 1;
         break;
@@ -352,10 +361,10 @@ __global__ void __launch_bounds__(128, 1)
     int kt = 0;
     const bool test_block = wait_test && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0;
     for (; kt < nk; ++kt) {
-      const int st = kt % TC_STAGES;
+      const int st = kt % nst;
       const bool ok = (test_block && kt == 0)
                           ? tc_mbar_wait(smem_u32(&never), 0, abort_v, 100000ull)
-                          : tc_mbar_wait(smem_u32(&full[st]), (kt / TC_STAGES) & 1, abort_v);
+                          : tc_mbar_wait(smem_u32(&full[st]), (kt / nst) & 1, abort_v);
       if (!__all_sync(0xffffffffu, ok && !*abort_v)) {
         if (lane == 0) *abort_v = 1;
         break;
@@ -395,7 +404,7 @@ __global__ void __launch_bounds__(128, 1)
     // loads issued but never consumed are still in flight: wait for them
     if (tid == 0) {
       for (int kt = n_seen; kt < n_loaded; ++kt)
-        tc_mbar_wait(smem_u32(&full[kt % TC_STAGES]), (kt / TC_STAGES) & 1);
+        tc_mbar_wait(smem_u32(&full[kt % nst]), (kt / nst) & 1);
       atomicAdd(err, 1);
     }
   } else {
@@ -778,23 +787,24 @@ void tc_launch(int bn, dim3 grid, cudaStream_t st, const CUtensorMap& ta, const 
                int M, int N, int K, float* C, int ldc, float alpha, float beta, int kc,
                float* work, int* err, TcEpi ep = TcEpi{}) {
   const int wt = g_gemm_wait_test;
+  const int ns = tc_ring_stages(kc);
   switch (bn) {
     case 32:
       if constexpr (!BMN)
-        k_gemm_tc<32, AMN, BMN, EPI><<<grid, 128, tc_smem_bytes(32), st>>>(
-            ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err, wt, ep);
+        k_gemm_tc<32, AMN, BMN, EPI><<<grid, 128, tc_smem_bytes(32, ns), st>>>(
+            ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err, wt, ep, ns);
       break;
     case 64:
-      k_gemm_tc<64, AMN, BMN, EPI><<<grid, 128, tc_smem_bytes(64), st>>>(
-          ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err, wt, ep);
+      k_gemm_tc<64, AMN, BMN, EPI><<<grid, 128, tc_smem_bytes(64, ns), st>>>(
+          ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err, wt, ep, ns);
       break;
     case 128:
-      k_gemm_tc<128, AMN, BMN, EPI><<<grid, 128, tc_smem_bytes(128), st>>>(
-          ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err, wt, ep);
+      k_gemm_tc<128, AMN, BMN, EPI><<<grid, 128, tc_smem_bytes(128, ns), st>>>(
+          ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err, wt, ep, ns);
       break;
     default:
-      k_gemm_tc<256, AMN, BMN, EPI><<<grid, 128, tc_smem_bytes(256), st>>>(
-          ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err, wt, ep);
+      k_gemm_tc<256, AMN, BMN, EPI><<<grid, 128, tc_smem_bytes(256, ns), st>>>(
+          ta, tb, M, N, K, C, ldc, alpha, beta, kc, work, err, wt, ep, ns);
   }
 }
 
