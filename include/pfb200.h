@@ -231,6 +231,11 @@ int pf_set_state(pf_engine *eng, int64_t step, const void *src, int64_t bytes,
  *                               sampled), then runs their n reverse steps
  *   pf_adj_read_grad(dst)       dJ/dK per cell, summed over Ex, Ey, Ez
  *                               (ncell doubles); dJ/deps_r = -K/eps_r dJ/dK.
+ *                               With one coefficient per cell (PF_CE_TABLE,
+ *                               PF_CE_CELL1) the reverse pass accumulates
+ *                               only this sum; with PF_CE_CELL3 it keeps
+ *                               the three components
+ *                               (pf_adj_read_grad_components).
  * The engine's current state afterwards is the end of the last replay. */
 int pf_adj_init(pf_engine *eng, int64_t ring_steps);
 int pf_adj_set_dft_cotangent(pf_engine *eng, int mon, const double *cot);

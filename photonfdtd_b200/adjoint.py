@@ -79,8 +79,10 @@ def _out_dict(res, torch):
 
 def _adjoint(sim, t: dict, loss: Callable, checkpoint_every) -> Tuple[float, np.ndarray]:
     """The forward run with checkpoints, the loss and its output
-    sensitivities, and the reverse pass: (J, dJ/dK_c) with the per-component
-    gradient shaped (3, *grid) for the E coefficients K of Ex, Ey, Ez."""
+    sensitivities, and the reverse pass: (J, dJ/dK) shaped (3, *grid), the
+    gradient per E coefficient K of Ex, Ey, Ez, when the tables give one
+    coefficient per component (PF_CE_CELL3); else shaped (1, *grid), the
+    sum over the components (all the reverse pass keeps then)."""
     import torch
     n_steps, dt = t["n_steps"], t["dt"]
     if n_steps < 1:
@@ -141,11 +143,13 @@ def _adjoint(sim, t: dict, loss: Callable, checkpoint_every) -> Tuple[float, np.
             buf = proxy.ckpts[s0]
             eng._chk(eng._L.pf_adj_segment(eng.h, int(s0), int(n), N.C.c_void_p(buf.data_ptr()),
                                            int(proxy.nbytes), 1))
-        grad_k = np.empty(3 * int(np.prod(t["shape"])), np.float64)
-        eng._chk(eng._L.pf_adj_read_grad_components(eng.h, N.ptr(grad_k, N.C.c_double)))
+        ncomp = 3 if t["ce_mode"] == N.PF_CE_CELL3 else 1
+        grad_k = np.empty(ncomp * int(np.prod(t["shape"])), np.float64)
+        read = (eng._L.pf_adj_read_grad_components if ncomp == 3 else eng._L.pf_adj_read_grad)
+        eng._chk(read(eng.h, N.ptr(grad_k, N.C.c_double)))
     finally:
         eng.close()
-    return value, grad_k.reshape((3,) + tuple(t["shape"]))
+    return value, grad_k.reshape((ncomp,) + tuple(t["shape"]))
 
 
 def _no_dispersion(sim, what: str) -> None:
@@ -172,7 +176,8 @@ def value_and_grad_eps(sim, loss: Callable, checkpoint_every: int = None
     dt = t["dt"]
     eps = np.asarray(sim.eps_r, dtype=np.float64).reshape(t["shape"])
     # K = dt / (eps0 eps_r) for all three components  =>  dK/deps_r = -dt / (eps0 eps_r^2)
-    grad = ((g3[0] + g3[1]) + g3[2]) * (-dt / (EPS_0 * eps * eps))
+    gk = g3[0] if g3.shape[0] == 1 else (g3[0] + g3[1]) + g3[2]
+    grad = gk * (-dt / (EPS_0 * eps * eps))
     return value, grad.astype(np.dtype(sim.dtypes["eps_r"]))
 
 

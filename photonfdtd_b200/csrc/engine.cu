@@ -1468,6 +1468,10 @@ AdjState<T> adj_state(pf_engine* e, long long slot) {
   }
   s.grad = e->grad;
   s.ncell = e->ncell;
+  // per-component coefficients are differentiated per component; one
+  // coefficient per cell needs only the sum (16 instead of 48 bytes of
+  // gradient traffic per cell and reverse step)
+  s.gstride = e->ce_mode == PF_CE_CELL3 ? e->ncell : 0;
   for (int a = 0; a < 3; ++a) s.idl[a] = (T)(1.0 / e->dl[a]);
   return s;
 }
@@ -1674,16 +1678,27 @@ int pf_adj_segment(pf_engine* e, int64_t step0, int64_t n, const void* state, in
 int pf_adj_read_grad_components(pf_engine* e, double* dst) {
   if (!e || !dst) return PF_ERR_INVALID;
   if (!e->adj) return fail(e, PF_ERR_STATE, "gradient read before pf_adj_init");
+  if (e->ce_mode != PF_CE_CELL3)
+    return fail(e, PF_ERR_STATE,
+                "per-component gradient kept only for per-component coefficients "
+                "(PF_CE_CELL3); use pf_adj_read_grad");
+  PF_CUDA(e, cudaSetDevice(e->device));
   PF_CUDA(e, cudaMemcpy(dst, e->grad, (size_t)e->ncell * 24, cudaMemcpyDeviceToHost));
   return PF_OK;
 }
 
 int pf_adj_read_grad(pf_engine* e, double* dst) {
   if (!e || !dst) return PF_ERR_INVALID;
-  std::vector<double> g((size_t)e->ncell * 3);
+  if (!e->adj) return fail(e, PF_ERR_STATE, "gradient read before pf_adj_init");
+  const size_t n = (size_t)e->ncell;
+  if (e->ce_mode != PF_CE_CELL3) {  // accumulated summed over the components
+    PF_CUDA(e, cudaSetDevice(e->device));
+    PF_CUDA(e, cudaMemcpy(dst, e->grad, n * 8, cudaMemcpyDeviceToHost));
+    return PF_OK;
+  }
+  std::vector<double> g(n * 3);
   int rc = pf_adj_read_grad_components(e, g.data());
   if (rc) return rc;
-  const size_t n = (size_t)e->ncell;
   for (size_t i = 0; i < n; ++i) dst[i] = (g[i] + g[n + i]) + g[2 * n + i];
   return PF_OK;
 }

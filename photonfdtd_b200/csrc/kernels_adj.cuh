@@ -39,8 +39,9 @@ struct AdjState {
   T* gH[6];   // of the H update: Hx A, Hx B, Hy A, Hy B, Hz A, Hz B
   T* lpE[6];  // psi adjoints (compact, like psiE / psiH)
   T* lpH[6];
-  double* grad;  // dJ/dK per component: Ex cells, then Ey, then Ez
+  double* grad;  // dJ/dK: per component (Ex cells, then Ey, then Ez) or summed
   long long ncell;
+  long long gstride;  // ncell: one gradient per component; 0: the three summed
   T idl[3];      // 1 / dl per axis
 };
 
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(256) k_adj_e(const __grid_constant__ StepArgs<
       if (qA >= 0) g = add_rn(g, s.psiErec[2 * c][qA]);
       if (qB >= 0) g = sub_rn(g, s.psiErec[2 * c + 1][qB]);
       const double gc = __dmul_rn((double)x, (double)g);
-      if (gc != 0.0) s.grad[c * s.ncell + id] = __dadd_rn(s.grad[c * s.ncell + id], gc);
+      if (gc != 0.0) s.grad[c * s.gstride + id] = __dadd_rn(s.grad[c * s.gstride + id], gc);
       curl_transpose<T>(x, K[c], rA, rB, qA, qB, rA ? a.be[axA][pos[axA]] : T(0),
                         rA ? a.cpe[axA][pos[axA]] : T(0), rB ? a.be[axB][pos[axB]] : T(0),
                         rB ? a.cpe[axB][pos[axB]] : T(0), s.lpE[2 * c], s.lpE[2 * c + 1], qa,
