@@ -106,28 +106,30 @@ def test_oracle_gradient_matches_central_differences(build, terms, seed):
         assert abs(fd - g[idx]) <= 1e-6 * gmax, (idx, fd, g[idx], gmax)
 
 
-def test_oracle_per_component_gradient_matches_central_differences():
+@pytest.mark.parametrize("build,terms", [(tiny3d, loss3d_terms), (tiny3d_flux, loss3d_flux_terms)])
+def test_oracle_per_component_gradient_matches_central_differences(build, terms):
     """dJ/dK_c for per-component E coefficients (the quantity
     value_and_grad_params chains to its parameters, jaxbackend.py:725-775):
-    an anisotropic coefficient set on the tiny 3D scene, against central
+    an anisotropic coefficient set on the tiny 3D scene (and with flux
+    terms in the loss), against central
     differences in single coefficients of each component."""
     from oracle.adjoint3d import value_and_grad_ce3
     from oracle.fdtd_oracle import EPS0, OracleRun
-    base = tiny3d()
+    base = build()
     eps = np.array(base.eps_r, dtype=np.float64)
     rng = np.random.default_rng(9)
     dt = OracleRun(base).dt
     ce3 = [dt / (EPS0 * eps * (1.0 + 0.2 * c) * (1.0 + 0.05 * rng.random(eps.shape)))
            for c in range(3)]
-    loss = scaled(tiny3d, loss3d_terms())
+    loss = scaled(build, terms())
 
     def value(c3):
-        r = OracleRun(tiny3d(), ce3=c3)
+        r = OracleRun(build(), ce3=c3)
         r.advance(r.n_steps)
         from oracle.adjoint3d import _out_dict
         return float(loss(_out_dict(r.result(), torch)).detach())
 
-    val, g3 = value_and_grad_ce3(tiny3d(), ce3, loss)
+    val, g3 = value_and_grad_ce3(build(), ce3, loss)
     assert val == pytest.approx(value(ce3), rel=1e-13)
     gmax = np.abs(g3).max()
     for comp in range(3):
