@@ -110,9 +110,9 @@ def test_oracle_gradient_matches_central_differences(build, terms, seed):
 def test_oracle_per_component_gradient_matches_central_differences(build, terms):
     """dJ/dK_c for per-component E coefficients (the quantity
     value_and_grad_params chains to its parameters, jaxbackend.py:725-775):
-    an anisotropic coefficient set on the tiny 3D scene (and with flux
-    terms in the loss), against central
-    differences in single coefficients of each component."""
+    an anisotropic coefficient set on the tiny 3D scene (also with flux
+    terms in the loss), against central differences in single coefficients
+    of each component."""
     from oracle.adjoint3d import value_and_grad_ce3
     from oracle.fdtd_oracle import EPS0, OracleRun
     base = build()
